@@ -1,0 +1,346 @@
+"""Benchmark of the checkerboard SU(2) sweep on one B200 (one JSON line).
+
+Workload (value): a 384^3 lattice with PMC boundary, hot start, one sweep =
+1 Kennedy-Pendleton heat-bath pass + 3 over-relaxation passes over the six
+checkerboard phases, FP32 links with FP64 fix-ups, links re-projected every
+sweep, energy/plaquette measured every 2 sweeps (N_cor = 2).  One step = one
+measurement interval = 2 sweeps + 1 measurement.  Metric = link updates/s,
+counting every heat-bath and over-relaxation update (12 V per sweep).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs an independent replica of the lattice (the sweep
+has no cross-replica exchange); value = all ranks' updates / max rank time.
+`--impl reference` times the reference's own kernels (mc_up_pmc + en_av from
+fezquerro/QCD_2d_GPU, built for sm_100a by oracle/Makefile) on the same
+lattice; the reference has no over-relaxation for PMC and no FP32 path, so its
+sweep is its heat-bath PMC sweep in FP64.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LT = LX = LY = 384
+BETA = 10.0
+N_OR = 3
+N_COR = 2
+L2_BYTES = 126 * 1024 * 1024
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples taken during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.p:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (getattr(self, "out", "") or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_cpu_baseline(seconds_hint: float = 20.0):
+    """The C oracle (the reference's FP64 sweep restated, own MRG32k3a, OpenMP
+    over all host cores) on a bounded sample: one 1 HB + 3 OR sweep of a
+    96 x 384 x 384 slab of the workload (a quarter of the lattice)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+
+    cores = po.set_threads(os.cpu_count() or 1)
+    lt = 96
+    o = po.Oracle(lt, LX, LY, BETA, algo=1, boundary=2, seed=1234)
+    o.init_hot()
+    t0 = time.perf_counter()
+    o.sweep(1)
+    o.overrelax(N_OR)
+    dt = time.perf_counter() - t0
+    o.close()
+    ups = 3.0 * lt * LX * LY * (1 + N_OR) / dt
+    return {"value": ups, "unit": "link updates/s", "cores": cores, "kind": "port",
+            "sample": f"1 sweep (1 HB + {N_OR} OR, FP64) of a {lt}x{LX}x{LY} PMC slab of the workload, "
+                      f"{dt:.1f} s"}
+
+
+def reference_arm(args, ws, rank):
+    if rank != 0:
+        return 0
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    base = {"impl": "reference", "metric": "link updates/s", "unit": "link updates/s",
+            "higher_is_better": True}
+    if not os.path.exists(harness):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/ref_harness not built (needs the reference checkout "
+                                         "at build time: make -C oracle ref)"}))
+        return 0
+    cmd = [harness, "bench", "--lt", str(LT), "--lx", str(LX), "--ly", str(LY), "--algo", "hb", "--bc", "2",
+           "--hot", "1", "--beta", str(BETA), "--sweeps", str(args.steps * N_COR), "--warmup",
+           str(args.warmup * N_COR)]
+    out = subprocess.run(cmd, capture_output=True, text=True, check=True)
+    r = json.loads(out.stdout.strip().splitlines()[-1])
+    sweeps = args.steps * N_COR
+    # one step = N_COR sweeps + one en_av measurement, as in our arm
+    step_ms = r["ms_per_sweep"] * N_COR + r["ms_measure"]
+    ups = 3.0 * LT * LX * LY * N_COR / (step_ms * 1e-3)
+    line = dict(base)
+    line.update({
+        "value": ups, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (hot start)",
+        "config": {"workload": f"{LT}x{LX}x{LY} PMC hot, reference sweep = heat-bath only (the reference "
+                               f"has no PMC over-relaxation and no FP32 path), FP64, measure every {N_COR} "
+                               "sweeps", "lattice": [LT, LX, LY], "boundary": "pmc", "precision": "fp64",
+                   "n_or": 0, "n_cor": N_COR, "l2": "inputs larger than L2 (5.4 GB link field)"},
+        "cpu_baseline": {"value": ups, "unit": "link updates/s", "cores": 1, "kind": "reference",
+                         "sample": f"reference kernels built for sm_100a on the B200, {sweeps} sweeps timed "
+                                   "with CUDA events (the reference has no CPU implementation)"},
+        "e2e": {"value": ups, "unit": "link updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_raw": r,
+    })
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lattice", type=int, nargs=3, default=None, help="override (testing only)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    ws, rank, local = dist_env()
+    if args.lattice:
+        global LT, LX, LY
+        LT, LX, LY = args.lattice
+
+    if args.impl == "reference":
+        return reference_arm(args, ws, rank)
+
+    import numpy as np
+    import torch
+
+    import qcd_2d_gpu_b200 as q
+
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    stream = torch.cuda.current_stream()
+    V = LT * LX * LY
+
+    L = q.Lattice(LT, LX, LY, BETA, algo="hb", boundary="pmc", precision="fp32", n_or=N_OR,
+                  renorm_every=1, seed=1234 + rank)
+    L.set_stream(stream.cuda_stream)
+    L.init_hot()
+
+    def step():
+        L.sweep(N_COR)
+        L.measure_into_series(0)
+
+    L.series_reserve(1)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    updates_per_step = 3.0 * V * (1 + N_OR) * N_COR
+    value = updates_per_step * args.steps * ws / (ms * 1e-3)
+    launches_per_step = N_COR * (6 * (1 + N_OR) + 1) + 1
+
+    # ---- dominant kernel: the over-relaxation phase, timed live ----------
+    # one qcd_overrelax pass = 6 launches of the OR phase kernel
+    reps = 5
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    L.overrelax(reps)
+    a1.record(stream)
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    L.close()
+    L2h = q.Lattice(LT, LX, LY, BETA, algo="hb", boundary="pmc", precision="fp32", n_or=0, seed=99)
+    L2h.set_stream(stream.cuda_stream)
+    torch.cuda.synchronize()
+    L2h.init_hot()
+    b0.record(stream)
+    L2h.sweep(reps)
+    b1.record(stream)
+    torch.cuda.synchronize()
+    or_launch_ms = a0.elapsed_time(a1) / (6 * reps)
+    hb_launch_ms = b0.elapsed_time(b1) / (6 * reps)
+    L2h.close()
+    vh = V // 2
+    or_bytes = 32.0 * vh  # strict: each FP32 link read once and written once
+    hb_bytes = 40.0 * vh  # + 2 x 24 B MRG32k3a state per 6 updates
+    hbm, peak_kind = peaks()
+    or_gbs = or_bytes / (or_launch_ms * 1e-3) / 1e9
+    roofline = {"kernel": "phase32<OR> (over-relaxation phase)", "bound": "hbm", "achieved": or_gbs,
+                "peak": hbm, "unit": "GB/s", "frac": or_gbs / hbm, "peak_source": peak_kind,
+                "traffic": None, "algorithmic_bytes_per_launch": or_bytes, "launch_ms": or_launch_ms,
+                "heatbath_phase": {"launch_ms": hb_launch_ms, "achieved": hb_bytes / (hb_launch_ms * 1e-3) / 1e9}}
+    traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(traffic_file):
+        try:
+            roofline["traffic"] = json.load(open(traffic_file)).get("phase32_or_bytes_per_launch")
+        except Exception:
+            pass
+
+    # ---- end to end through the C ABI with host buffers -------------------
+    # one host configuration in the reference's AoS FP64 layout is uploaded
+    # (pinned host -> device, converted to FP32 SoA) at the start of the timed
+    # region; every step reads its (energy, plaquette) back to the host.
+    host_cfg = torch.empty(V * 12, dtype=torch.float64, pin_memory=True)
+    hv = host_cfg.numpy()
+    hv[:] = 0.0
+    hv[0::4] = 1.0  # a cold configuration
+    E = q.Lattice(LT, LX, LY, BETA, algo="hb", boundary="pmc", precision="fp32", n_or=N_OR,
+                  renorm_every=1, seed=4321 + rank)
+    E.set_stream(stream.cuda_stream)
+    E.load_config(hv)  # allocate the staging buffer outside the timed region
+    E.sweep(N_COR)
+    E.measure()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    E.load_config(hv)
+    for _ in range(args.steps):
+        E.sweep(N_COR)
+        E.measure()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = t0.elapsed_time(t1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = updates_per_step * args.steps * ws / (e2e_ms * 1e-3)
+    E.close()
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = run_cpu_baseline()
+
+    if rank == 0:
+        line = {
+            "metric": "link updates/s",
+            "value": value,
+            "unit": "link updates/s",
+            "n_gpus": ws,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32+f64-fixups",
+            "data": "synthetic (hot start, seeded MRG32k3a)",
+            "config": {"workload": f"{LT}x{LX}x{LY} PMC, hot start, sweep = 1 heat-bath + {N_OR} "
+                                   f"over-relaxation, FP32 links + FP64 fix-ups, renormalise every sweep, "
+                                   f"measure every {N_COR} sweeps",
+                       "lattice": [LT, LX, LY], "boundary": "pmc", "precision": "fp32", "n_or": N_OR,
+                       "n_cor": N_COR, "beta": BETA,
+                       "l2": f"inputs larger than L2 ({V * 48 / 1e9:.2f} GB FP32 link store)",
+                       "parallelism": f"replicas x{ws}"},
+            "hb_link_updates_per_s": 3.0 * V * N_COR * args.steps * ws / (ms * 1e-3),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "link updates/s",
+                    "h2d_bytes_per_step": V * 12 * 8 / args.steps, "d2h_bytes_per_step": 16,
+                    "note": "one AoS FP64 configuration uploaded from pinned host memory per timed run "
+                            "(amortised over the steps); one (energy, plaquette) readback per step"},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

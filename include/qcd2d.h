@@ -1,0 +1,188 @@
+/*
+ * qcd2d.h — C ABI of the B200-native checkerboard SU(2) Wilson-action sweep.
+ *
+ * Drop-in for the hot path of fezquerro/QCD_2d_GPU (2+1-D SU(2) lattice gauge
+ * theory, links stored as unit quaternions).  The reference has no library
+ * boundary: its host program kernel.cu calls device-buffer launchers
+ * (`mc_up_per/pcc/pmc`, `normalize`, `en_av`, `setup_kernel`, the init
+ * kernels) directly from main().  Each entry point below replaces one of those
+ * call sites; the citation on each declaration names it (file:line of the
+ * reference).  Device memory is owned by the library, host buffers by the
+ * caller.  One lattice handle = one CUDA stream; a handle is not thread-safe.
+ * Every function returns QCD_OK (0) or a negative qcd_status; the message of
+ * the last failure on a handle is qcd_last_error(h).
+ *
+ * Layout at the boundary (qcd_load_config / qcd_store_config) is the
+ * reference's: V*12 doubles, site-major, even sublattice first
+ * (site = id for even sites, id + V/2 for odd sites, id = y' + (Ly/2)*(x + Lx*t)),
+ * 3 links per site in the order y, x, t, 4 quaternion components each
+ * (kernel.cu:58, lattice_setup.h:24-37, output.h:77-94).
+ */
+#ifndef QCD2D_H
+#define QCD2D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+enum qcd_status {
+  QCD_OK = 0,
+  QCD_ERR_INVALID = -1,     /* bad argument: odd or zero size, bad enum, null pointer */
+  QCD_ERR_CUDA = -2,        /* a CUDA runtime call failed (message in qcd_last_error) */
+  QCD_ERR_NOMEM = -3,       /* device allocation failed */
+  QCD_ERR_NONUNITARY = -4,  /* a link's determinant is far from 1 or not finite */
+  QCD_ERR_TIMEOUT = -5,     /* a bounded device-side wait ran out */
+  QCD_ERR_IO = -6,          /* configuration file missing, short or malformed */
+  QCD_ERR_UNSUPPORTED = -7  /* combination not provided (e.g. FP32 Metropolis in parity mode) */
+};
+
+/* update algorithm: values of kernel.cu:11-12 (METROPOLIS 0, HEATBATH 1) */
+enum qcd_algo { QCD_ALGO_METROPOLIS = 0, QCD_ALGO_HEATBATH = 1 };
+
+/* y boundary condition: values of kernel.cu:28 (Boundary) */
+enum qcd_boundary { QCD_BC_PERIODIC = 0, QCD_BC_PCC = 1, QCD_BC_PMC = 2 };
+
+/* link storage / arithmetic */
+enum qcd_precision {
+  /* FP64 links and the reference's exact operation order and RNG draw order:
+     reproduces the reference link field (max|dU| <= 1e-12 after 10 sweeps) */
+  QCD_PREC_FP64 = 0,
+  /* FP32 links and FP32 staples / heat-bath / over-relaxation; FP64 kept for the
+     Kennedy-Pendleton a0 near 1, the Metropolis exact fallback, link
+     re-projection and the global plaquette/energy sums */
+  QCD_PREC_FP32 = 1
+};
+
+/* Parameters of one lattice.  Mirrors `struct lattice` (lattice_setup.h:2-14)
+   and the #define knobs of kernel.cu:11-46 that concern the sweep. */
+typedef struct qcd_params {
+  int lt, lx, ly;          /* d_t, d_x, d_y (kernel.cu:24-26); all even and >= 2 */
+  float beta;              /* betal (kernel.cu:27); float like lattice.beta */
+  float epsilon;           /* epsilonl (kernel.cu:43), Metropolis proposal size */
+  int upd;                 /* upd (kernel.cu:44), Metropolis hits per link */
+  int algo;                /* enum qcd_algo (kernel.cu:13) */
+  int boundary;            /* enum qcd_boundary (kernel.cu:28) */
+  int precision;           /* enum qcd_precision */
+  int n_or;                /* over-relaxation passes after each heat-bath/Metropolis
+                              pass inside qcd_sweep (0 = the reference's sweep) */
+  int renorm_every;        /* re-project all links every this many qcd_sweep sweeps
+                              (0 = never inside qcd_sweep; the host calls
+                              qcd_normalize, as kernel.cu:163,203 does) */
+  unsigned long long seed; /* seed of the MRG32k3a streams (lattice_setup.h:15-21) */
+} qcd_params;
+
+typedef struct qcd_lattice qcd_lattice;
+
+/* Fill p with the reference's defaults for an Lt x Lx x Ly lattice. */
+void qcd_params_default(qcd_params* p, int lt, int lx, int ly);
+
+/* Allocate the link store, the V/2 MRG32k3a streams (curand_init(seed, id, 0),
+   replaces setup_kernel, kernel.cu:77-79 / lattice_setup.h:15-21) and the
+   measurement buffers.  Rejects odd sizes like kernel.cu:61-64. */
+int qcd_create(const qcd_params* p, qcd_lattice** out);
+int qcd_destroy(qcd_lattice* h);
+
+/* Launch everything on `stream` (a cudaStream_t); NULL restores the handle's
+   own stream. */
+int qcd_set_stream(qcd_lattice* h, void* stream);
+/* The cudaStream_t the handle currently launches on. */
+void* qcd_get_stream(qcd_lattice* h);
+
+/* Cold start: all links = 1 (id_init2, lattice_setup.h:38-51; kernel.cu:94). */
+int qcd_init_cold(qcd_lattice* h);
+/* Hot start: 4 uniform doubles in (-0.5,0.5] per link, normalised, drawn from
+   stream id in the order even y,x,t then odd y,x,t (rand_init2,
+   lattice_setup.h:24-37); with PCC the x,t links at y=0 stay 1 and draw
+   nothing (rand_init2_pcc, lattice_setup.h:52-81; kernel.cu:91,108,125). */
+int qcd_init_hot(qcd_lattice* h);
+
+/* Configuration in the reference's AoS FP64 layout (see top of file).
+   Host buffers: read_conf + cudaMemcpy H2D (lattice_setup.h:83-100,
+   kernel.cu:98-99) and cudaMemcpy D2H + save_conf (kernel.cu:183-185,
+   output.h:77-94).  FP32 lattices convert at the boundary. */
+int qcd_load_config(qcd_lattice* h, const double* aos_host);
+int qcd_store_config(qcd_lattice* h, double* aos_host);
+/* Same with device buffers of V*12 doubles (no host copy). */
+int qcd_load_config_device(qcd_lattice* h, const double* aos_dev);
+int qcd_store_config_device(qcd_lattice* h, double* aos_dev);
+
+/* n full sweeps.  One sweep = the 6 checkerboard phases even_y, odd_y, even_x,
+   odd_x, even_t, odd_t with heat-bath or `upd` Metropolis hits per link
+   (mc_up_per mc_updates.h:467-475, mc_up_pcc mc_updates_pcc.h:216-224,
+   mc_up_pmc mc_updates_pmc.h:249-257; called at kernel.cu:166-170,196-200),
+   then n_or over-relaxation passes, then re-projection if renorm_every says so. */
+int qcd_sweep(qcd_lattice* h, int n);
+/* n over-relaxation passes over the 6 phases (mc_up_per(..., update=1),
+   mc_updates.h:109-115,178-181; extended to PCC/PMC with the same masks). */
+int qcd_overrelax(qcd_lattice* h, int n);
+/* Re-project every link onto SU(2) (normalize, lattice_setup.h:202-207;
+   kernel.cu:163-164,179,203-204). */
+int qcd_normalize(qcd_lattice* h);
+
+/* Energy = mean over sites of -(1 - P_xt) and average plaquette
+   = mean of (P_yx + P_yt + P_xt)/3, PMC counting the y-plaquettes at
+   y = Ly-1 as 1 (en_av<PMC>, observables.h:99-141; kernel.cu:208).
+   FP64 sums in a fixed order: the result does not depend on scheduling.
+   Synchronous: waits for the stream. */
+int qcd_measure(qcd_lattice* h, double* energy, double* plaquette);
+/* Asynchronous form: writes (energy, plaquette) into slot `index` of the
+   handle's device series (capacity set by qcd_series_reserve); read the
+   series back with qcd_series_read. */
+int qcd_series_reserve(qcd_lattice* h, int capacity);
+int qcd_measure_into_series(qcd_lattice* h, int index);
+int qcd_series_read(qcd_lattice* h, double* energy, double* plaquette, int n);
+
+/* Accepted updates per site since the last reset, V ints in the reference's
+   site order (the `accept` array of kernel.cu:144-145, filled by
+   link_update mc_updates.h:119-128 and read by mean_lattice,
+   statistics.h:17-28).  Heat-bath and over-relaxation count 1 per link. */
+int qcd_accept_counts(qcd_lattice* h, int* host_out);
+int qcd_accept_reset(qcd_lattice* h);
+
+/* Check that every link has |det - 1| <= tol and is finite; returns
+   QCD_ERR_NONUNITARY otherwise (the device writes a flag, nothing traps).
+   The mean determinant (print_det, lattice_setup.h:176-183) goes to *mean_det
+   when it is not NULL. */
+int qcd_check_unitarity(qcd_lattice* h, double tol, double* mean_det);
+
+/* Lattice facts. */
+long long qcd_volume(const qcd_lattice* h);
+int qcd_get_params(const qcd_lattice* h, qcd_params* out);
+/* Device pointer and byte size of the link store (diagnostics, benchmarks). */
+int qcd_link_store(const qcd_lattice* h, void** dev_ptr, size_t* bytes);
+
+const char* qcd_last_error(const qcd_lattice* h);
+const char* qcd_status_string(int status);
+
+/* ------------------------------------------------------------------------
+ * Random-number tape.  For stream id in [first, first+n_streams), seeded as
+ * curand_init(seed, id, 0) exactly like setup_kernel (lattice_setup.h:15-21),
+ * record the first n_draws draws.  Draw k is taken both as curand_uniform
+ * and as curand_uniform_double from the same generator position, with the
+ * CUDA float values the reference's heat-bath applies to one draw
+ * (logf, cospif(2u), sincospif(2u); mc_updates.h:47-55).  `same_step` is 1
+ * when both flavours advanced the generator identically.  Host-side replays
+ * (the CPU oracle) consume this instead of re-implementing the generator.
+ * ------------------------------------------------------------------------ */
+typedef struct qcd_tape_record {
+  double ud;
+  float uf;
+  float log_uf;
+  float cospi_2uf;
+  float sc_sin;
+  float sc_cos;
+  unsigned int same_step;
+} qcd_tape_record;
+
+int qcd_rng_tape(unsigned long long seed, long long first, int n_streams, int n_draws,
+                 qcd_tape_record* host_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QCD2D_H */
