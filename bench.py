@@ -191,7 +191,11 @@ def main():
         from datetime import timedelta
 
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library launches on it and the CUDA events are
+    # recorded on it (torch's default stream is the legacy stream 0, which does
+    # not order work on the library's own non-blocking stream)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     V = LT * LX * LY
 
     L = q.Lattice(LT, LX, LY, BETA, algo="hb", boundary="pmc", precision="fp32", n_or=N_OR,
