@@ -181,6 +181,37 @@ typedef struct qcd_tape_record {
 int qcd_rng_tape(unsigned long long seed, long long first, int n_streams, int n_draws,
                  qcd_tape_record* host_out);
 
+/* ------------------------------------------------------------------------
+ * Measurement that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory when they measure: a
+ * program that sized its lattice to fill the GPU, one whose device memory
+ * belongs to the pooling allocator of its host framework, or a sweep loop
+ * that cannot take the implicit device synchronisation of cudaMalloc /
+ * cudaFree.  It needs no handle: it reads a configuration the caller holds
+ * in device memory in the reference's AoS FP64 layout (V*12 doubles, the
+ * layout of kernel.cu's `phid`, 16-byte aligned) and writes
+ * out_dev[0] = energy, out_dev[1] = average plaquette (same definitions,
+ * per-site arithmetic and summation order as qcd_measure) asynchronously on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream).  It calls no
+ * cudaMalloc, cudaFree or other allocating routine: its reduction scratch is
+ * a fixed array inside the library, present on every GPU that loads it until
+ * the process exits.
+ *
+ * Limit: V/2 <= QCD_NOALLOC_MAX_HALF_SITES (V <= 8,388,608, e.g. 192^3);
+ * larger lattices return QCD_ERR_UNSUPPORTED (and say so on stderr) — use
+ * qcd_measure on a handle for those.
+ * The first call on a device looks up the scratch array's device address
+ * (with lazy module loading it also loads the library's kernels there); make
+ * that first call before any stream capture.  All calls share the one
+ * scratch array: calls that can overlap on the GPU (different streams, no
+ * ordering between them) race and must not be issued.
+ * ------------------------------------------------------------------------ */
+#define QCD_NOALLOC_MAX_BLOCKS 16384
+#define QCD_NOALLOC_MAX_HALF_SITES (QCD_NOALLOC_MAX_BLOCKS * 256)
+int qcd_measure_aos_noalloc(const double* phi_dev, int lt, int lx, int ly, int boundary,
+                            double* out_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -122,6 +122,7 @@ _SIGS = {
     "qcd_last_error": (ctypes.c_char_p, [_P]),
     "qcd_status_string": (ctypes.c_char_p, [_I]),
     "qcd_rng_tape": (_I, [ctypes.c_ulonglong, ctypes.c_longlong, _I, _I, _P]),
+    "qcd_measure_aos_noalloc": (_I, [_P, _I, _I, _I, _I, _P, _P]),
 }
 
 

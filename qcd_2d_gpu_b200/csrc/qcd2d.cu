@@ -8,6 +8,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <mutex>
 #include <new>
 #include "kernels.cuh"
 #include "qcd2d.h"
@@ -566,3 +567,112 @@ int qcd_rng_tape(unsigned long long seed, long long first, int n_streams, int n_
 }
 
 }  // extern "C"
+
+// ======================================================== no allocation ==
+// Measurement of a caller-held configuration that allocates nothing: the
+// reduction scratch (one partial sum per CTA and the arrival counter) is the
+// file-scope array below instead of cudaMalloc'd memory.  A program that has
+// sized its lattice to fill the GPU, or whose device memory belongs to the
+// pooling allocator of its host framework, or whose sweep loop cannot take
+// the implicit device synchronisation of cudaMalloc/cudaFree, can still
+// measure.  The kernel is measure<> (same per-site arithmetic, CTA size and
+// summation order as qcd_measure) reading the reference's AoS FP64 layout.
+namespace qcd {
+
+struct LinksAoS {
+  const double* phi;  // V*12 doubles: site (p*Vh + id), link d, component c
+  int vh;
+  __device__ __forceinline__ Quat<double> ld(int d, int p, int id) const {
+    const double* s = phi + ((size_t)p * vh + id) * 12 + d * 4;
+    double2 a = __ldg(reinterpret_cast<const double2*>(s));
+    double2 b = __ldg(reinterpret_cast<const double2*>(s + 2));
+    return Quat<double>{a.x, a.y, b.x, b.y};
+  }
+};
+template <>
+__device__ __forceinline__ Quat<double> ld64<LinksAoS>(const LinksAoS& links, int d, int p, int id) {
+  return links.ld(d, p, id);
+}
+
+}  // namespace qcd
+
+// partial sums of at most QCD_NOALLOC_MAX_BLOCKS CTAs, then the arrival counter
+static constexpr size_t kNoAllocCounterOffset = (size_t)QCD_NOALLOC_MAX_BLOCKS * sizeof(double2);
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocCounterOffset + 256];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[256];  // device address of g_noalloc_scratch, per device ordinal
+
+// Host code may not use g_noalloc_scratch itself (on the host it names a
+// stand-in, not device memory): look up its device address once per device,
+// with that device current.
+int noalloc_scratch(void** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 256) {
+    cudaGetLastError();
+    return QCD_ERR_CUDA;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      fprintf(stderr, "qcd_measure_aos_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", dev,
+              cudaGetErrorString(e));
+      return QCD_ERR_CUDA;
+    }
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return QCD_OK;
+}
+}  // namespace
+
+extern "C" int qcd_measure_aos_noalloc(const double* phi_dev, int lt, int lx, int ly, int boundary,
+                                       double* out_dev, void* stream) {
+  if (!phi_dev || !out_dev) return QCD_ERR_INVALID;
+  if (lt < 2 || lx < 2 || ly < 2 || (lt & 1) || (lx & 1) || (ly & 1)) return QCD_ERR_INVALID;
+  if (boundary < 0 || boundary > 2) return QCD_ERR_INVALID;
+  if (((uintptr_t)phi_dev & 15) || ((uintptr_t)out_dev & 7)) return QCD_ERR_INVALID;
+  const long long vh = (long long)lt * lx * ly / 2;
+  const long long nb = (vh + kBlock - 1) / kBlock;
+  if (vh > QCD_NOALLOC_MAX_HALF_SITES || nb > QCD_NOALLOC_MAX_BLOCKS) {
+    fprintf(stderr,
+            "qcd_measure_aos_noalloc: %dx%dx%d has V/2 = %lld sites, above the %d that its fixed "
+            "scratch holds; use qcd_measure on a handle instead\n",
+            lt, lx, ly, vh, QCD_NOALLOC_MAX_HALF_SITES);
+    return QCD_ERR_UNSUPPORTED;
+  }
+  void* base = nullptr;
+  int rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  double2* partials = reinterpret_cast<double2*>(base);
+  unsigned int* counter = reinterpret_cast<unsigned int*>(static_cast<char*>(base) + kNoAllocCounterOffset);
+  cudaStream_t s = (cudaStream_t)stream;
+  // the array keeps whatever the previous call left: the arrival counter must start at zero
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), s);
+  if (e == cudaSuccess) {
+    Geo g;
+    g.lt = lt;
+    g.lx = lx;
+    g.ly = ly;
+    g.lyh = ly / 2;
+    g.slice = g.lyh * lx;
+    g.vh = (int)vh;
+    LinksAoS L{phi_dev, (int)vh};
+    if (boundary == QCD_BC_PMC)
+      measure<LinksAoS, 1><<<(unsigned int)nb, kBlock, 0, s>>>(L, g, partials, counter, out_dev);
+    else
+      measure<LinksAoS, 0><<<(unsigned int)nb, kBlock, 0, s>>>(L, g, partials, counter, out_dev);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    fprintf(stderr, "qcd_measure_aos_noalloc: %s\n", cudaGetErrorString(e));
+    return QCD_ERR_CUDA;
+  }
+  return QCD_OK;
+}

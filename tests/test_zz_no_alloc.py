@@ -1,0 +1,82 @@
+"""qcd_measure_aos_noalloc: the measurement for callers that cannot allocate.
+
+Such a caller (a lattice that fills the GPU, device memory owned by a host
+framework's pool, a loop that must not synchronise on cudaMalloc/cudaFree)
+holds its configuration in device memory in the reference's AoS layout and
+gets energy and plaquette back without the library allocating anything.
+This file runs last so that a failure here cannot hide the other tests.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import qcd_2d_gpu_b200 as q
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-14  # same summation order as qcd_measure: equal up to the last bit
+
+
+def _dev_ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+@pytest.mark.parametrize("bc", [0, 1, 2])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_noalloc_matches_measure_on_two_calls(bc, precision):
+    import torch
+
+    lib = q.load_library()
+    lt, lx, ly = 8, 6, 10
+    L = q.Lattice(lt, lx, ly, 7.0, boundary=bc, precision=precision, seed=99 + bc)
+    L.init_hot()
+    L.sweep(3)
+    phi = torch.empty(lt * lx * ly * 12, dtype=torch.float64, device="cuda")
+    assert lib.qcd_store_config_device(L.handle, _dev_ptr(phi)) == 0
+    e_ref, p_ref = L.measure()  # synchronises the handle's stream
+    torch.cuda.synchronize()
+    out = torch.empty(2, dtype=torch.float64, device="cuda")
+    for _ in range(2):  # the scratch keeps the previous call's contents
+        out.fill_(float("nan"))
+        torch.cuda.synchronize()
+        rc = lib.qcd_measure_aos_noalloc(_dev_ptr(phi), lt, lx, ly, bc, _dev_ptr(out), None)
+        assert rc == 0
+        torch.cuda.synchronize()
+        e, p = out.cpu().tolist()
+        assert abs(e - e_ref) <= TOL and abs(p - p_ref) <= TOL
+    L.close()
+
+
+def test_noalloc_allocates_nothing_after_first_call():
+    import torch
+
+    lib = q.load_library()
+    lt = lx = ly = 16
+    L = q.Lattice(lt, lx, ly, 6.0, seed=5)
+    L.init_cold()
+    L.sweep(2)
+    phi = torch.empty(lt * lx * ly * 12, dtype=torch.float64, device="cuda")
+    out = torch.empty(2, dtype=torch.float64, device="cuda")
+    assert lib.qcd_store_config_device(L.handle, _dev_ptr(phi)) == 0
+    ref = L.measure()
+    torch.cuda.synchronize()
+    assert lib.qcd_measure_aos_noalloc(_dev_ptr(phi), lt, lx, ly, 0, _dev_ptr(out), None) == 0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(5):
+        assert lib.qcd_measure_aos_noalloc(_dev_ptr(phi), lt, lx, ly, 0, _dev_ptr(out), None) == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert np.allclose(out.cpu().numpy(), ref, rtol=0, atol=TOL)
+    L.close()
+
+
+def test_noalloc_rejects_lattices_beyond_its_scratch():
+    lib = q.load_library()
+    # 384^3 has V/2 = 28,311,552 > QCD_NOALLOC_MAX_HALF_SITES: refused on the host,
+    # before any device access (the pointers are never dereferenced)
+    fake = ctypes.c_void_p(256)
+    assert lib.qcd_measure_aos_noalloc(fake, 384, 384, 384, 2, fake, None) == -7
+    assert lib.qcd_measure_aos_noalloc(fake, 8, 7, 8, 0, fake, None) == -1  # odd extent
+    assert lib.qcd_measure_aos_noalloc(None, 8, 8, 8, 0, fake, None) == -1
