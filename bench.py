@@ -264,7 +264,7 @@ def main():
                 "peak": hbm, "unit": "GB/s", "frac": or_gbs / hbm, "peak_source": peak_kind,
                 "traffic": None, "algorithmic_bytes_per_launch": or_bytes, "launch_ms": or_launch_ms,
                 "heatbath_phase": {"launch_ms": hb_launch_ms, "achieved": hb_bytes / (hb_launch_ms * 1e-3) / 1e9}}
-    traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
+    traffic_file = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(traffic_file):
         try:
             roofline["traffic"] = json.load(open(traffic_file)).get("phase32_or_bytes_per_launch")

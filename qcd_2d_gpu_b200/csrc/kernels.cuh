@@ -19,16 +19,19 @@ struct PhaseArgs {
   int upd;
   int* err;     // device error word
   int* accept;  // V ints, reference site order; only for Metropolis
+  int renorm;   // FP32: re-project each updated link (in double) before it is stored
 };
 
 // ------------------------------------------------------------ one phase --
 // Update U_MU on sublattice PAR: one of the six launches of mc_up_per/pcc/pmc
 // (mc_updates.h:129-465, mc_updates_pcc.h:4-214, mc_updates_pmc.h:4-247).
+// Launch grid (ceil(slice / kBlock), Lt): blockIdx.y is the t-slice.
 template <int MU, int PAR, int BC, int KIND>
 __global__ void __launch_bounds__(kBlock) phase64(Links64 L, RngStore R, Geo g, PhaseArgs a) {
-  const int id = blockIdx.x * kBlock + threadIdx.x;
-  if (id >= g.vh) return;
-  const Nbr n = make_nbr(g, id, PAR);
+  const int s = blockIdx.x * kBlock + threadIdx.x;
+  if (s >= g.slice) return;
+  const Nbr n = make_nbr_slice(g, s, blockIdx.y, PAR);
+  const int id = n.id;
   if (BC == BC_PCC && MU != DIR_Y && at_y0(g, n)) return;
   Quat<double> A = staple_sum<MU, BC, Links64, double>(L, g, n, PAR);
   if (KIND == KIND_HB) {
@@ -53,28 +56,29 @@ __global__ void __launch_bounds__(kBlock) phase64(Links64 L, RngStore R, Geo g, 
 
 template <int MU, int PAR, int BC, int KIND>
 __global__ void __launch_bounds__(kBlock) phase32(Links32 L, RngStore R, Geo g, PhaseArgs a) {
-  const int id = blockIdx.x * kBlock + threadIdx.x;
-  if (id >= g.vh) return;
-  const Nbr n = make_nbr(g, id, PAR);
+  const int s = blockIdx.x * kBlock + threadIdx.x;
+  if (s >= g.slice) return;
+  const Nbr n = make_nbr_slice(g, s, blockIdx.y, PAR);
+  const int id = n.id;
   if (BC == BC_PCC && MU != DIR_Y && at_y0(g, n)) return;
   Quat<float> A = staple_sum<MU, BC, Links32, float>(L, g, n, PAR);
+  Quat<float> U;
   if (KIND == KIND_HB) {
     curandStateMRG32k3a_t st;
     R.load(id, &st);
-    L.st(MU, PAR, id, heatbath_fast(A, a.beta, &st, a.err));
+    U = heatbath_fast(A, a.beta, &st, a.err);
     R.store(id, &st);
   } else if (KIND == KIND_METRO) {
     curandStateMRG32k3a_t st;
     R.load(id, &st);
-    Quat<float> U = L.ld_own(MU, PAR, id);
+    U = L.ld_own(MU, PAR, id);
     int acc = metropolis_fast(U, A, a.beta, a.eps, a.upd, &st);
-    L.st(MU, PAR, id, U);
     R.store(id, &st);
     a.accept[PAR * g.vh + id] += acc;
   } else {
-    Quat<float> U = L.ld_own(MU, PAR, id);
-    L.st(MU, PAR, id, overrelax_fast(A, U));
+    U = overrelax_fast(A, L.ld_own(MU, PAR, id));
   }
+  L.st(MU, PAR, id, a.renorm ? renorm_fast(U) : U);
 }
 
 // ------------------------------------------------------------ RNG setup --

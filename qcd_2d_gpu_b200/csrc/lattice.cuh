@@ -27,7 +27,24 @@ struct Geo {
   int lyh;         // Ly / 2
   int slice;       // Lyh * Lx : sublattice sites per t-slice
   int vh;          // Lyh * Lx * Lt
+  // s / lyh for 0 <= s < slice as (s * lyh_magic) >> 32, lyh_magic = ceil(2^32 / lyh):
+  // exact when lyh^2 * lx < 2^32 (fastdiv = 1), otherwise a hardware division is used
+  unsigned long long lyh_magic;
+  int fastdiv;
 };
+
+__host__ __forceinline__ Geo make_geo(int lt, int lx, int ly) {
+  Geo g;
+  g.lt = lt;
+  g.lx = lx;
+  g.ly = ly;
+  g.lyh = ly / 2;
+  g.slice = g.lyh * lx;
+  g.vh = g.slice * lt;
+  g.lyh_magic = ((1ull << 32) + (unsigned long long)g.lyh - 1) / (unsigned long long)g.lyh;
+  g.fastdiv = (unsigned long long)g.lyh * (unsigned long long)g.lyh * (unsigned long long)lx < (1ull << 32);
+  return g;
+}
 
 // Decoded sublattice site plus the offsets (in sublattice index units) of its
 // six neighbours, which all lie on the other sublattice.  Offsets add: the
@@ -39,6 +56,9 @@ struct Nbr {
   int yp, ym, xp, xm, tp, tm;
 };
 
+__device__ __forceinline__ void finish_nbr(const Geo& g, int parity, Nbr& n);
+
+// From the sublattice index (two divisions).
 __device__ __forceinline__ Nbr make_nbr(const Geo& g, int id, int parity) {
   Nbr n;
   n.id = id;
@@ -46,6 +66,23 @@ __device__ __forceinline__ Nbr make_nbr(const Geo& g, int id, int parity) {
   int r = id / g.lyh;
   n.x = r % g.lx;
   n.t = r / g.lx;
+  finish_nbr(g, parity, n);
+  return n;
+}
+
+// From the position s inside t-slice t (launch grid (slice, Lt)): one
+// multiply-high instead of two divisions.
+__device__ __forceinline__ Nbr make_nbr_slice(const Geo& g, int s, int t, int parity) {
+  Nbr n;
+  n.t = t;
+  n.x = g.fastdiv ? (int)(((unsigned long long)(unsigned)s * g.lyh_magic) >> 32) : s / g.lyh;
+  n.yq = s - n.x * g.lyh;
+  n.id = s + t * g.slice;
+  finish_nbr(g, parity, n);
+  return n;
+}
+
+__device__ __forceinline__ void finish_nbr(const Geo& g, int parity, Nbr& n) {
   n.q = ((n.t + n.x) & 1) ^ parity;
   // +y: a site with odd physical y moves to the next y' (wrapping), an even
   // one stays at the same y' (mc_updates.h:139-141, 195-197)
@@ -56,7 +93,6 @@ __device__ __forceinline__ Nbr make_nbr(const Geo& g, int id, int parity) {
   n.xm = n.x == 0 ? (g.lx - 1) * g.lyh : -g.lyh;
   n.tp = n.t == g.lt - 1 ? -(g.lt - 1) * g.slice : g.slice;
   n.tm = n.t == 0 ? (g.lt - 1) * g.slice : -g.slice;
-  return n;
 }
 
 __device__ __forceinline__ int off_plus(const Nbr& n, int dir) {

@@ -134,15 +134,16 @@ Phase32Fn phase_fn32(int k, int bc, int kind) {
   }
 }
 
-// one pass over the six phases with one update kind
-int pass(qcd_lattice* h, int kind) {
-  PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept};
-  const unsigned int nb = nblocks(h->g.vh);
+// one pass over the six phases with one update kind; with `renorm` (FP32
+// only) every link is re-projected as it is stored
+int pass(qcd_lattice* h, int kind, int renorm = 0) {
+  PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, renorm};
+  const dim3 grid(nblocks(h->g.slice), (unsigned int)h->g.lt);
   for (int k = 0; k < 6; k++) {
     if (h->p.precision == QCD_PREC_FP64)
-      phase_fn64(k, h->p.boundary, kind)<<<nb, kBlock, 0, h->stream>>>(links64(h), rngs(h), h->g, a);
+      phase_fn64(k, h->p.boundary, kind)<<<grid, kBlock, 0, h->stream>>>(links64(h), rngs(h), h->g, a);
     else
-      phase_fn32(k, h->p.boundary, kind)<<<nb, kBlock, 0, h->stream>>>(links32(h), rngs(h), h->g, a);
+      phase_fn32(k, h->p.boundary, kind)<<<grid, kBlock, 0, h->stream>>>(links32(h), rngs(h), h->g, a);
     LAUNCH_CHECK(h);
   }
   if (kind != KIND_METRO) h->unit_passes++;
@@ -261,12 +262,7 @@ int qcd_create(const qcd_params* p, qcd_lattice** out) {
   if (!h) return QCD_ERR_NOMEM;
   h->p = *p;
   h->V = V;
-  h->g.lt = p->lt;
-  h->g.lx = p->lx;
-  h->g.ly = p->ly;
-  h->g.lyh = p->ly / 2;
-  h->g.slice = h->g.lyh * p->lx;
-  h->g.vh = (int)(V / 2);
+  h->g = make_geo(p->lt, p->lx, p->ly);
   const size_t vh = (size_t)h->g.vh;
   int rc = QCD_OK;
   auto step = [&](cudaError_t e, const char* what) {
@@ -414,11 +410,16 @@ int qcd_sweep(qcd_lattice* h, int n) {
   if (!h || n < 0) return QCD_ERR_INVALID;
   const int kind = h->p.algo == QCD_ALGO_HEATBATH ? KIND_HB : KIND_METRO;
   for (int i = 0; i < n; i++) {
-    int rc = pass(h, kind);
-    for (int r = 0; rc == QCD_OK && r < h->p.n_or; r++) rc = pass(h, KIND_OR);
+    const bool renorm = h->p.renorm_every > 0 && (h->sweeps_done + 1) % h->p.renorm_every == 0;
+    // FP32: the re-projection rides on the sweep's last pass, each link being
+    // re-projected at its last update (no extra read of the store); FP64
+    // keeps the reference's separate normalize after the sweep
+    const bool fused = renorm && h->p.precision == QCD_PREC_FP32;
+    int rc = pass(h, kind, fused && h->p.n_or == 0);
+    for (int r = 0; rc == QCD_OK && r < h->p.n_or; r++) rc = pass(h, KIND_OR, fused && r == h->p.n_or - 1);
     if (rc) return rc;
     h->sweeps_done++;
-    if (h->p.renorm_every > 0 && h->sweeps_done % h->p.renorm_every == 0) {
+    if (renorm && !fused) {
       rc = qcd_normalize(h);
       if (rc) return rc;
     }
@@ -655,13 +656,7 @@ extern "C" int qcd_measure_aos_noalloc(const double* phi_dev, int lt, int lx, in
   // the array keeps whatever the previous call left: the arrival counter must start at zero
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), s);
   if (e == cudaSuccess) {
-    Geo g;
-    g.lt = lt;
-    g.lx = lx;
-    g.ly = ly;
-    g.lyh = ly / 2;
-    g.slice = g.lyh * lx;
-    g.vh = (int)vh;
+    Geo g = make_geo(lt, lx, ly);
     LinksAoS L{phi_dev, (int)vh};
     if (boundary == QCD_BC_PMC)
       measure<LinksAoS, 1><<<(unsigned int)nb, kBlock, 0, s>>>(L, g, partials, counter, out_dev);

@@ -164,8 +164,10 @@ __device__ __forceinline__ Quat<float> heatbath_fast(Quat<float> A, float beta,
   float aux;
   for (int tries = 1;; tries++) {
     float r0 = curand_uniform(st), r1 = curand_uniform(st), r2 = curand_uniform(st);
-    float c = cospif(2.f * r1);
-    lf = -(logf(r0) + c * c * logf(r2)) * inv;
+    // hardware approximations (absolute error ~2^-21): cos(2 pi r1) evaluated
+    // as -cos(2 pi (r1 - 1/2)) keeps the argument in [-pi, pi]
+    float c = -__cosf(6.2831853f * (r1 - 0.5f));
+    lf = -(__logf(r0) + c * c * __logf(r2)) * inv;
     aux = 1.f - curand_uniform(st);
     if (!((double)aux * aux > 1.0 - (double)lf)) break;
     if (tries >= QCD_HB_MAX_TRIES) {
@@ -177,9 +179,9 @@ __device__ __forceinline__ Quat<float> heatbath_fast(Quat<float> A, float beta,
   float x0 = (float)(1.0 - 2.0 * lfd);
   float nrm = (float)(2.0 * sqrt(lfd * (1.0 - lfd)));
   float ct = 2.f * curand_uniform(st) - 1.f, sp, cp;
-  sincospif(2.f * curand_uniform(st), &sp, &cp);
+  __sincosf(6.2831853f * (curand_uniform(st) - 0.5f), &sp, &cp);  // angle + pi
   float stt = sqrtf(fmaxf(0.f, 1.f - ct * ct));
-  Quat<float> X{x0, nrm * ct, nrm * stt * cp, nrm * stt * sp};
+  Quat<float> X{x0, nrm * ct, -nrm * stt * cp, -nrm * stt * sp};
   return q_mul_bd(X, A);
 }
 
