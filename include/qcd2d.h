@@ -149,6 +149,39 @@ int qcd_accept_reset(qcd_lattice* h);
    when it is not NULL. */
 int qcd_check_unitarity(qcd_lattice* h, double tol, double* mean_det);
 
+/* ------------------------------------------------------------------------
+ * Scheduling of the six checkerboard phases (replaces the reference's six
+ * serial launches per sweep, mc_updates.h:467-475, with the same result).
+ *   PHASES     one launch per phase: each phase streams the link store.
+ *   WAVEFRONT  one persistent launch per chain of passes: every t-slice goes
+ *              through the phases of the chain while it is resident in L2;
+ *              tasks run in a ring schedule ordered so that each waits only
+ *              for earlier ones (bounded waits, QCD_ERR_TIMEOUT otherwise).
+ *              Bit-identical to PHASES.
+ *   AUTO       the schedule measured fastest for the lattice (currently PHASES).
+ * ------------------------------------------------------------------------ */
+enum qcd_schedule { QCD_SCHED_AUTO = 0, QCD_SCHED_PHASES = 1, QCD_SCHED_WAVEFRONT = 2 };
+int qcd_set_schedule(qcd_lattice* h, int mode);
+/* the schedule qcd_sweep will use (PHASES or WAVEFRONT) */
+int qcd_get_schedule(const qcd_lattice* h);
+/* Wavefront knobs (0 keeps the current value): sites per task (rounded up to
+   a multiple of 256), passes chained per launch (1..4; more passes keep more
+   slices live in L2) and fronts (a divisor of Lt leaving arcs of >= 2 slices:
+   the ring is cut into that many arcs that advance together, multiplying the
+   ready tasks and the live slices).  Defaults: 256 sites, as many passes as
+   keep the live slices within ~64 MB, 1 front. */
+int qcd_set_wave_tuning(qcd_lattice* h, int chunk_sites, int passes_per_launch, int fronts);
+/* Host-only planner of the wavefront (no GPU): for a program of n_phases
+   phases (mu[n] in {0 y, 1 x, 2 t}, par[n] in {0, 1}) writes each phase's
+   seam slice, start step and, in need[o*n_phases + n] (o = 0, 1, 2 for slice
+   offsets -1, 0, +1), the latest earlier phase it waits for (-1: none). */
+int qcd_wave_plan(const int* mu, const int* par, int n_phases, int* seam, int* start, int* need);
+/* Self-test of the bounded waits: one wavefront pass in which the first task
+   waits for a count no task produces; expected result QCD_ERR_TIMEOUT, with
+   the CUDA context still usable (the links of that pass are left partly
+   updated: re-initialise the lattice afterwards). */
+int qcd_wave_selftest_timeout(qcd_lattice* h);
+
 /* Lattice facts. */
 long long qcd_volume(const qcd_lattice* h);
 int qcd_get_params(const qcd_lattice* h, qcd_params* out);

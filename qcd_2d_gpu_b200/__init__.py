@@ -31,6 +31,7 @@ LIB_PATH = os.path.join(_HERE, "libqcd2d.so")
 METROPOLIS, HEATBATH = 0, 1
 PERIODIC, PCC, PMC = 0, 1, 2
 FP64, FP32 = 0, 1
+SCHED_AUTO, SCHED_PHASES, SCHED_WAVEFRONT = 0, 1, 2
 
 _BC = {"periodic": PERIODIC, "per": PERIODIC, "pcc": PCC, "pmc": PMC}
 _ALGO = {"metropolis": METROPOLIS, "metro": METROPOLIS, "heatbath": HEATBATH, "hb": HEATBATH}
@@ -123,6 +124,11 @@ _SIGS = {
     "qcd_status_string": (ctypes.c_char_p, [_I]),
     "qcd_rng_tape": (_I, [ctypes.c_ulonglong, ctypes.c_longlong, _I, _I, _P]),
     "qcd_measure_aos_noalloc": (_I, [_P, _I, _I, _I, _I, _P, _P]),
+    "qcd_set_schedule": (_I, [_P, _I]),
+    "qcd_get_schedule": (_I, [_P]),
+    "qcd_wave_plan": (_I, [_P, _P, _I, _P, _P, _P]),
+    "qcd_wave_selftest_timeout": (_I, [_P]),
+    "qcd_set_wave_tuning": (_I, [_P, _I, _I, _I]),
 }
 
 
@@ -225,6 +231,21 @@ class Lattice:
     def set_stream(self, stream_ptr: int | None) -> None:
         self._check(self._lib.qcd_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)), "set_stream")
 
+    def set_schedule(self, mode: int | str) -> None:
+        m = {"auto": SCHED_AUTO, "phases": SCHED_PHASES, "wavefront": SCHED_WAVEFRONT}.get(mode, mode)
+        self._check(self._lib.qcd_set_schedule(self._h, int(m)), "set_schedule")
+
+    def schedule(self) -> str:
+        return {SCHED_PHASES: "phases", SCHED_WAVEFRONT: "wavefront"}[self._lib.qcd_get_schedule(self._h)]
+
+    def set_wave_tuning(self, chunk_sites: int = 0, passes_per_launch: int = 0, fronts: int = 0) -> None:
+        self._check(self._lib.qcd_set_wave_tuning(self._h, chunk_sites, passes_per_launch, fronts),
+                    "set_wave_tuning")
+
+    def wave_selftest_timeout(self) -> int:
+        """Run the bounded-wait self-test; returns the status (expected -5)."""
+        return self._lib.qcd_wave_selftest_timeout(self._h)
+
     # -- the path ---------------------------------------------------------
     def init_cold(self) -> None:
         self._check(self._lib.qcd_init_cold(self._h), "init_cold")
@@ -297,3 +318,18 @@ def rng_tape(seed: int, first: int, n_streams: int, n_draws: int, lib: ctypes.CD
     if rc != QCD_OK:
         raise QcdError(rc, "qcd_rng_tape")
     return out.reshape(n_streams, n_draws)
+
+
+def wave_plan(mu, par, lib: ctypes.CDLL | None = None):
+    """Host-side wavefront plan (seam, start, need[3][P]) of a phase program."""
+    lib = lib or load_library()
+    m = np.ascontiguousarray(mu, dtype=np.int32)
+    p = np.ascontiguousarray(par, dtype=np.int32)
+    n = len(m)
+    seam = np.zeros(n, np.int32)
+    start = np.zeros(n, np.int32)
+    need = np.zeros(3 * n, np.int32)
+    rc = lib.qcd_wave_plan(_ptr(m), _ptr(p), n, _ptr(seam), _ptr(start), _ptr(need))
+    if rc != QCD_OK:
+        raise QcdError(rc, "qcd_wave_plan")
+    return seam, start, need.reshape(3, n)

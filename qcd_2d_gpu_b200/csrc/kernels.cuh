@@ -22,18 +22,25 @@ struct PhaseArgs {
   int renorm;   // FP32: re-project each updated link (in double) before it is stored
 };
 
-// ------------------------------------------------------------ one phase --
-// Update U_MU on sublattice PAR: one of the six launches of mc_up_per/pcc/pmc
-// (mc_updates.h:129-465, mc_updates_pcc.h:4-214, mc_updates_pmc.h:4-247).
-// Launch grid (ceil(slice / kBlock), Lt): blockIdx.y is the t-slice.
-template <int MU, int PAR, int BC, int KIND>
-__global__ void __launch_bounds__(kBlock) phase64(Links64 L, RngStore R, Geo g, PhaseArgs a) {
-  const int s = blockIdx.x * kBlock + threadIdx.x;
-  if (s >= g.slice) return;
-  const Nbr n = make_nbr_slice(g, s, blockIdx.y, PAR);
-  const int id = n.id;
+// ------------------------------------------------------- one link update --
+// Update U_MU at site n of sublattice PAR: the body of the six launches of
+// mc_up_per/pcc/pmc (mc_updates.h:129-465, mc_updates_pcc.h:4-214,
+// mc_updates_pmc.h:4-247).  Shared by the per-phase kernels (CG = false) and
+// the wavefront kernel (CG = true).
+template <bool CG>
+__device__ __forceinline__ void add_accept(int* p, int v) {
+  if (CG)
+    atomicAdd(p, v);  // at L2: the counter may sit in a stale L1 line
+  else
+    *p += v;
+}
+
+template <int MU, int PAR, int BC, int KIND, bool CG>
+__device__ __forceinline__ void site64(const Links64T<CG>& L, const RngStoreT<CG>& R, const Geo& g,
+                                       const PhaseArgs& a, const Nbr& n) {
   if (BC == BC_PCC && MU != DIR_Y && at_y0(g, n)) return;
-  Quat<double> A = staple_sum<MU, BC, Links64, double>(L, g, n, PAR);
+  const int id = n.id;
+  Quat<double> A = staple_sum<MU, BC, Links64T<CG>, double>(L, g, n, PAR);
   if (KIND == KIND_HB) {
     curandStateMRG32k3a_t st;
     R.load(id, &st);
@@ -47,21 +54,19 @@ __global__ void __launch_bounds__(kBlock) phase64(Links64 L, RngStore R, Geo g, 
     int acc = metropolis_ref(U, A, (double)a.beta, (double)a.eps, a.upd, &st);
     L.st(MU, PAR, id, U);
     R.store(id, &st);
-    a.accept[PAR * g.vh + id] += acc;
+    add_accept<CG>(a.accept + PAR * g.vh + id, acc);
   } else {
     Quat<double> U = L.ld_own(MU, PAR, id);
     L.st(MU, PAR, id, overrelax_ref(A, U));
   }
 }
 
-template <int MU, int PAR, int BC, int KIND>
-__global__ void __launch_bounds__(kBlock) phase32(Links32 L, RngStore R, Geo g, PhaseArgs a) {
-  const int s = blockIdx.x * kBlock + threadIdx.x;
-  if (s >= g.slice) return;
-  const Nbr n = make_nbr_slice(g, s, blockIdx.y, PAR);
-  const int id = n.id;
+template <int MU, int PAR, int BC, int KIND, bool CG>
+__device__ __forceinline__ void site32(const Links32T<CG>& L, const RngStoreT<CG>& R, const Geo& g,
+                                       const PhaseArgs& a, const Nbr& n, int renorm) {
   if (BC == BC_PCC && MU != DIR_Y && at_y0(g, n)) return;
-  Quat<float> A = staple_sum<MU, BC, Links32, float>(L, g, n, PAR);
+  const int id = n.id;
+  Quat<float> A = staple_sum<MU, BC, Links32T<CG>, float>(L, g, n, PAR);
   Quat<float> U;
   if (KIND == KIND_HB) {
     curandStateMRG32k3a_t st;
@@ -74,11 +79,27 @@ __global__ void __launch_bounds__(kBlock) phase32(Links32 L, RngStore R, Geo g, 
     U = L.ld_own(MU, PAR, id);
     int acc = metropolis_fast(U, A, a.beta, a.eps, a.upd, &st);
     R.store(id, &st);
-    a.accept[PAR * g.vh + id] += acc;
+    add_accept<CG>(a.accept + PAR * g.vh + id, acc);
   } else {
     U = overrelax_fast(A, L.ld_own(MU, PAR, id));
   }
-  L.st(MU, PAR, id, a.renorm ? renorm_fast(U) : U);
+  L.st(MU, PAR, id, renorm ? renorm_fast(U) : U);
+}
+
+// ------------------------------------------------------------ one phase --
+// Launch grid (ceil(slice / kBlock), Lt): blockIdx.y is the t-slice.
+template <int MU, int PAR, int BC, int KIND>
+__global__ void __launch_bounds__(kBlock) phase64(Links64 L, RngStore R, Geo g, PhaseArgs a) {
+  const int s = blockIdx.x * kBlock + threadIdx.x;
+  if (s >= g.slice) return;
+  site64<MU, PAR, BC, KIND, false>(L, R, g, a, make_nbr_slice(g, s, blockIdx.y, PAR));
+}
+
+template <int MU, int PAR, int BC, int KIND>
+__global__ void __launch_bounds__(kBlock) phase32(Links32 L, RngStore R, Geo g, PhaseArgs a) {
+  const int s = blockIdx.x * kBlock + threadIdx.x;
+  if (s >= g.slice) return;
+  site32<MU, PAR, BC, KIND, false>(L, R, g, a, make_nbr_slice(g, s, blockIdx.y, PAR), a.renorm);
 }
 
 // ------------------------------------------------------------ RNG setup --

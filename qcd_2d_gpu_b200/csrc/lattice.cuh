@@ -110,44 +110,71 @@ __device__ __forceinline__ bool at_ytop(const Geo& g, const Nbr& n) {
 
 __host__ __device__ __forceinline__ size_t plane_of(int dir, int parity) { return (size_t)(dir * 2 + parity); }
 
+// Load/store policy: CG = false uses the read-only path (__ldg) for neighbour
+// links, which is safe inside one phase launch because no link a phase reads
+// is written in that launch.  CG = true (the wavefront kernel) reads and
+// writes at L2 (.cg): there, other CTAs of the same launch rewrite links, and
+// a line left in this SM's L1 by an earlier task could be stale.
+template <class T, bool CG>
+__device__ __forceinline__ T ld_nb(const T* p) {
+  if (CG) return __ldcg(p);
+  return __ldg(p);
+}
+template <class T, bool CG>
+__device__ __forceinline__ T ld_rw(const T* p) {
+  if (CG) return __ldcg(p);
+  return *p;
+}
+template <class T, bool CG>
+__device__ __forceinline__ void st_rw(T* p, const T& v) {
+  if (CG)
+    __stcg(p, v);
+  else
+    *p = v;
+}
+
 // ---------------------------------------------------------------- FP64 ----
-struct Links64 {
+template <bool CG>
+struct Links64T {
   double2* lo;  // (w, x)
   double2* hi;  // (y, z)
   int vh;
   __device__ __forceinline__ Quat<double> ld(int dir, int parity, int id) const {
     size_t i = plane_of(dir, parity) * vh + id;
-    double2 a = __ldg(lo + i), b = __ldg(hi + i);
+    double2 a = ld_nb<double2, CG>(lo + i), b = ld_nb<double2, CG>(hi + i);
     return Quat<double>{a.x, a.y, b.x, b.y};
   }
-  // coherent load for the link this thread rewrites
+  // the link this thread rewrites
   __device__ __forceinline__ Quat<double> ld_own(int dir, int parity, int id) const {
     size_t i = plane_of(dir, parity) * vh + id;
-    double2 a = lo[i], b = hi[i];
+    double2 a = ld_rw<double2, CG>(lo + i), b = ld_rw<double2, CG>(hi + i);
     return Quat<double>{a.x, a.y, b.x, b.y};
   }
   __device__ __forceinline__ void st(int dir, int parity, int id, const Quat<double>& u) const {
     size_t i = plane_of(dir, parity) * vh + id;
-    lo[i] = make_double2(u.w, u.x);
-    hi[i] = make_double2(u.y, u.z);
+    st_rw<double2, CG>(lo + i, make_double2(u.w, u.x));
+    st_rw<double2, CG>(hi + i, make_double2(u.y, u.z));
   }
 };
+typedef Links64T<false> Links64;
 
 // ---------------------------------------------------------------- FP32 ----
-struct Links32 {
+template <bool CG>
+struct Links32T {
   float4* q;
   int vh;
   __device__ __forceinline__ Quat<float> ld(int dir, int parity, int id) const {
-    float4 a = __ldg(q + plane_of(dir, parity) * vh + id);
+    float4 a = ld_nb<float4, CG>(q + plane_of(dir, parity) * vh + id);
     return Quat<float>{a.x, a.y, a.z, a.w};
   }
   __device__ __forceinline__ Quat<float> ld_own(int dir, int parity, int id) const {
-    float4 a = q[plane_of(dir, parity) * vh + id];
+    float4 a = ld_rw<float4, CG>(q + plane_of(dir, parity) * vh + id);
     return Quat<float>{a.x, a.y, a.z, a.w};
   }
   __device__ __forceinline__ void st(int dir, int parity, int id, const Quat<float>& u) const {
-    q[plane_of(dir, parity) * vh + id] = make_float4(u.w, u.x, u.y, u.z);
+    st_rw<float4, CG>(q + plane_of(dir, parity) * vh + id, make_float4(u.w, u.x, u.y, u.z));
   }
 };
+typedef Links32T<false> Links32;
 
 }  // namespace qcd

@@ -12,6 +12,7 @@
 #include <new>
 #include "kernels.cuh"
 #include "qcd2d.h"
+#include "wave.cuh"
 
 using namespace qcd;
 
@@ -43,6 +44,18 @@ struct qcd_lattice {
   // conversion staging for host configs
   double* aos_stage = nullptr;
   long long sweeps_done = 0;
+  // wavefront scheduler
+  int sched = QCD_SCHED_AUTO;
+  unsigned int* wave_done = nullptr;   // Lt arrival counters
+  unsigned int* wave_queue = nullptr;  // ticket counter
+  int* wave_abort = nullptr;
+  int wave_grid = 0;                   // persistent CTAs (all SMs x occupancy)
+  int wave_chain = 0;                  // passes chained per launch (0: not planned yet)
+  int wave_chunk = 256;                // sites per wavefront task
+  int wave_fronts = 1;                 // ring fronts (arcs of Lt / fronts slices)
+  unsigned int* wave_tasks[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // per chain length
+  int wave_tasks_chunk[5] = {0, 0, 0, 0, 0};
+  int wave_tasks_fronts[5] = {0, 0, 0, 0, 0};
   char msg[512] = {0};
 };
 
@@ -150,12 +163,280 @@ int pass(qcd_lattice* h, int kind, int renorm = 0) {
   return QCD_OK;
 }
 
+// ------------------------------------------------------------ wavefront --
+// Link classes are (direction, parity); a phase of type (mu, p) writes class
+// (mu, p) of its own slice and reads the classes below at slice offsets
+// -1, 0, +1 (the staple sites of mc_updates.h:158-176 and its siblings; the
+// PMC masks only remove reads, so this superset is safe for every boundary).
+struct ClassRef {
+  int dir, par, off;
+};
+
+int read_set(int mu, int p, ClassRef* r) {
+  int k = 0;
+  const int q = 1 - p;
+  if (mu != DIR_T) {
+    const int nu = 1 - mu;  // the other spatial direction
+    const ClassRef v[] = {{nu, p, 0}, {nu, q, 0}, {mu, q, 0}, {mu, q, 1}, {mu, q, -1},
+                          {DIR_T, q, 0}, {DIR_T, p, 0}, {DIR_T, p, -1}, {DIR_T, q, -1}, {mu, p, 0}};
+    for (const ClassRef& c : v) r[k++] = c;
+  } else {
+    for (int nu = DIR_Y; nu <= DIR_X; nu++) {
+      const ClassRef v[] = {{nu, q, 1}, {nu, p, 0}, {nu, p, 1}, {nu, q, 0}};
+      for (const ClassRef& c : v) r[k++] = c;
+    }
+    r[k++] = ClassRef{DIR_T, q, 0};
+    r[k++] = ClassRef{DIR_T, p, 0};
+  }
+  return k;
+}
+
+bool reads(int mu, int p, int dir, int par, int off) {
+  ClassRef r[16];
+  const int k = read_set(mu, p, r);
+  for (int i = 0; i < k; i++)
+    if (r[i].dir == dir && r[i].par == par && r[i].off == off) return true;
+  return false;
+}
+
+// must phase m at slice t+o finish before phase n at slice t?
+bool conflict(int mu_m, int p_m, int mu_n, int p_n, int o) {
+  return reads(mu_n, p_n, mu_m, p_m, o) ||   // n reads what m wrote
+         reads(mu_m, p_m, mu_n, p_n, -o) ||  // m reads what n overwrites
+         (mu_m == mu_n && p_m == p_n && o == 0);
+}
+
+// Seam s_n and start T_n of each phase: the seam advances (by one slice) only
+// where a dependency on slice t-1 needs it, and T_n is the earliest start that
+// keeps every conflicting task of an earlier phase at a strictly earlier time
+// step for every t of the ring: T_n - T_m >= (s_n - s_m) + o + 1.
+int plan_wave(const int* mu, const int* par, int P, short need[3][kMaxWavePhases], int* seam, int* start) {
+  if (P < 1 || P > kMaxWavePhases) return QCD_ERR_INVALID;
+  for (int n = 0; n < P; n++) {
+    for (int o = -1; o <= 1; o++) {
+      int best = -1;
+      for (int m = 0; m < n; m++)
+        if (conflict(mu[m], par[m], mu[n], par[n], o)) best = m;
+      need[o + 1][n] = (short)best;
+    }
+  }
+  seam[0] = 0;
+  start[0] = 0;
+  for (int n = 1; n < P; n++) {
+    seam[n] = seam[n - 1];
+    for (int m = 0; m < n; m++)
+      if (conflict(mu[m], par[m], mu[n], par[n], -1) && seam[n] - seam[m] < 1) seam[n] = seam[m] + 1;
+    int lo = start[n - 1] + 1;
+    for (int m = 0; m < n; m++)
+      for (int o = -1; o <= 1; o++)
+        if (conflict(mu[m], par[m], mu[n], par[n], o)) {
+          const int d = seam[n] - seam[m];
+          if (d + o < 0) return QCD_ERR_INVALID;  // cannot happen with the seam rule above
+          lo = lo > start[m] + d + o + 1 ? lo : start[m] + d + o + 1;
+        }
+    start[n] = lo;
+  }
+  return QCD_OK;
+}
+
+struct PassSpec {
+  int kind;    // KIND_HB / KIND_METRO / KIND_OR
+  int renorm;  // FP32: re-project each link as this pass stores it
+};
+
+constexpr unsigned int kWaveSpin = 1u << 22;  // ~1 s of polling per wait
+
+// slices kept live by a chain of `passes` passes (the L2 working set)
+int wave_window(int passes) {
+  int mu[kMaxWavePhases], par[kMaxWavePhases], seam[kMaxWavePhases], start[kMaxWavePhases];
+  short need[3][kMaxWavePhases];
+  const int P = 6 * passes;
+  for (int n = 0; n < P; n++) {
+    mu[n] = (n % 6) / 2;
+    par[n] = n % 2;
+  }
+  plan_wave(mu, par, P, need, seam, start);
+  return (start[P - 1] - seam[P - 1]) - (start[0] - seam[0]) + 3;
+}
+
+template <class L, int BC, int SK>
+void* wave_fn() {
+  return (void*)wave<L, BC, SK>;
+}
+
+void* pick_wave(int prec, int bc, int sk) {
+  if (prec == QCD_PREC_FP64) {
+    if (sk == KIND_HB)
+      return bc == 0 ? wave_fn<Links64T<true>, 0, KIND_HB>() : bc == 1 ? wave_fn<Links64T<true>, 1, KIND_HB>()
+                                                                    : wave_fn<Links64T<true>, 2, KIND_HB>();
+    return bc == 0 ? wave_fn<Links64T<true>, 0, KIND_METRO>() : bc == 1 ? wave_fn<Links64T<true>, 1, KIND_METRO>()
+                                                                       : wave_fn<Links64T<true>, 2, KIND_METRO>();
+  }
+  if (sk == KIND_HB)
+    return bc == 0 ? wave_fn<Links32T<true>, 0, KIND_HB>() : bc == 1 ? wave_fn<Links32T<true>, 1, KIND_HB>()
+                                                                  : wave_fn<Links32T<true>, 2, KIND_HB>();
+  return bc == 0 ? wave_fn<Links32T<true>, 0, KIND_METRO>() : bc == 1 ? wave_fn<Links32T<true>, 1, KIND_METRO>()
+                                                                     : wave_fn<Links32T<true>, 2, KIND_METRO>();
+}
+
+int wave_setup(qcd_lattice* h) {
+  if (h->wave_chain) return QCD_OK;
+  if (!h->wave_done) CUDA_OR_FAIL(h, cudaMalloc(&h->wave_done, (size_t)h->g.lt * sizeof(unsigned int)));
+  if (!h->wave_queue) CUDA_OR_FAIL(h, cudaMalloc(&h->wave_queue, sizeof(unsigned int)));
+  if (!h->wave_abort) CUDA_OR_FAIL(h, cudaMalloc(&h->wave_abort, sizeof(int)));
+  int dev = 0, sms = 0, per_sm = 0;
+  CUDA_OR_FAIL(h, cudaGetDevice(&dev));
+  CUDA_OR_FAIL(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int sk = h->p.algo == QCD_ALGO_HEATBATH ? KIND_HB : KIND_METRO;
+  CUDA_OR_FAIL(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_wave(h->p.precision, h->p.boundary, sk),
+                                                                 kBlock, 0));
+  h->wave_grid = sms * (per_sm > 0 ? per_sm : 1);
+  // chain as many passes per launch as keep the live slices within ~64 MB of L2
+  const double slice_bytes =
+      (double)h->g.slice * (6.0 * (h->p.precision == QCD_PREC_FP64 ? 32.0 : 16.0) + 24.0);
+  int chain = 1;
+  while (chain < kMaxWavePhases / 6 && wave_window(chain + 1) * slice_bytes <= 64.0 * 1024 * 1024) chain++;
+  h->wave_chain = chain;
+  return QCD_OK;
+}
+
+// Ticket order of a chain of np passes: tasks sorted by time step, then by
+// phase, arc and chunk.  With K fronts the ring of Lt slices is cut into K
+// arcs of L' = Lt/K slices that advance together:
+//     tau(n, t) = T_n + ((t - s_n) mod L').
+// The conditions on (s_n, T_n) only involve slice offsets -1..+1 modulo the
+// period, so a plan valid for a ring of L' >= 2 slices is valid for every arc
+// at once; K fronts give K times the ready tasks and K times the live slices.
+int wave_task_table(qcd_lattice* h, int np, const WaveSched& S, int fronts, const unsigned int** out) {
+  if (h->wave_tasks[np] && h->wave_tasks_chunk[np] == S.chunk_sites && h->wave_tasks_fronts[np] == fronts) {
+    *out = h->wave_tasks[np];
+    return QCD_OK;
+  }
+  const int lt = S.lt, arc = S.lt / fronts;
+  unsigned int* host = (unsigned int*)malloc((size_t)S.n_tasks * sizeof(unsigned int));
+  if (!host) return fail(h, QCD_ERR_NOMEM, "wavefront task table");
+  size_t k = 0;
+  const int steps = S.start[S.P - 1] + arc;
+  for (int tau = 0; tau < steps; tau++)
+    for (int n = 0; n < S.P; n++) {
+      if (tau < S.start[n] || tau >= S.start[n] + arc) continue;
+      const int u = (S.seam[n] + (tau - S.start[n])) % arc;
+      for (int a = 0; a < fronts; a++)
+        for (int c = 0; c < S.chunks; c++) host[k++] = wave_pack(n, c, a * arc + u);
+    }
+  (void)lt;
+  cudaError_t e = cudaSuccess;
+  if (k != S.n_tasks) {
+    free(host);
+    return fail(h, QCD_ERR_INVALID, "wavefront task table has %zu of %u tasks", k, S.n_tasks);
+  }
+  if (h->wave_tasks[np]) cudaFree(h->wave_tasks[np]);
+  h->wave_tasks[np] = nullptr;
+  e = cudaMalloc(&h->wave_tasks[np], (size_t)S.n_tasks * sizeof(unsigned int));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(h->wave_tasks[np], host, (size_t)S.n_tasks * sizeof(unsigned int), cudaMemcpyHostToDevice);
+  free(host);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(h, QCD_ERR_CUDA, "wavefront task table: %s", cudaGetErrorString(e));
+  }
+  h->wave_tasks_chunk[np] = S.chunk_sites;
+  h->wave_tasks_fronts[np] = fronts;
+  *out = h->wave_tasks[np];
+  return QCD_OK;
+}
+
+int launch_wave(qcd_lattice* h, const PassSpec* ps, int np, int stall_test = 0,
+                unsigned int spin = kWaveSpin) {
+  int rc = wave_setup(h);
+  if (rc) return rc;
+  WaveSched S;
+  memset(&S, 0, sizeof(S));
+  int mu[kMaxWavePhases], par[kMaxWavePhases];
+  S.P = 6 * np;
+  if (np < 1 || S.P > kMaxWavePhases) return fail(h, QCD_ERR_INVALID, "wavefront program of %d passes", np);
+  for (int n = 0; n < S.P; n++) {
+    mu[n] = (n % 6) / 2;
+    par[n] = n % 2;
+    S.mu[n] = (signed char)mu[n];
+    S.par[n] = (signed char)par[n];
+    S.kind[n] = (signed char)ps[n / 6].kind;
+    S.renorm[n] = (signed char)ps[n / 6].renorm;
+  }
+  rc = plan_wave(mu, par, S.P, S.need, S.seam, S.start);
+  if (rc) return fail(h, rc, "wavefront plan failed");
+  S.lt = h->g.lt;
+  S.chunk_sites = h->g.slice < h->wave_chunk ? h->g.slice : h->wave_chunk;
+  S.chunks = (h->g.slice + S.chunk_sites - 1) / S.chunk_sites;
+  S.n_tasks = (unsigned int)S.P * (unsigned int)S.lt * (unsigned int)S.chunks;
+  S.n_steps = S.start[S.P - 1] + S.lt;
+  if (S.chunks > 4096 || h->g.lt >= 32768)
+    return fail(h, QCD_ERR_UNSUPPORTED, "wavefront task words hold at most 4096 chunks and 32767 slices");
+  const unsigned int* tasks = nullptr;
+  const int fronts = (h->wave_fronts >= 1 && h->g.lt % h->wave_fronts == 0 && h->g.lt / h->wave_fronts >= 2)
+                         ? h->wave_fronts
+                         : 1;
+  rc = wave_task_table(h, np, S, fronts, &tasks);
+  if (rc) return rc;
+  WaveCtl c{h->wave_done, h->wave_queue, h->wave_abort, tasks, spin, stall_test};
+  CUDA_OR_FAIL(h, cudaMemsetAsync(h->wave_done, 0, (size_t)h->g.lt * sizeof(unsigned int), h->stream));
+  CUDA_OR_FAIL(h, cudaMemsetAsync(h->wave_queue, 0, sizeof(unsigned int), h->stream));
+  CUDA_OR_FAIL(h, cudaMemsetAsync(h->wave_abort, 0, sizeof(int), h->stream));
+  PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, 0};
+  const int sk = h->p.algo == QCD_ALGO_HEATBATH ? KIND_HB : KIND_METRO;
+  const int bc = h->p.boundary;
+  const unsigned int grid = (unsigned int)h->wave_grid;
+  RngStoreT<true> R{h->rng, h->g.vh};
+  if (h->p.precision == QCD_PREC_FP64) {
+    Links64T<true> L{h->lo, h->hi, h->g.vh};
+    if (sk == KIND_HB) {
+      if (bc == 0) wave<Links64T<true>, 0, KIND_HB><<<grid, kBlock, 0, h->stream>>>(L, R, h->g, a, S, c);
+      else if (bc == 1) wave<Links64T<true>, 1, KIND_HB><<<grid, kBlock, 0, h->stream>>>(L, R, h->g, a, S, c);
+      else wave<Links64T<true>, 2, KIND_HB><<<grid, kBlock, 0, h->stream>>>(L, R, h->g, a, S, c);
+    } else {
+      if (bc == 0) wave<Links64T<true>, 0, KIND_METRO><<<grid, kBlock, 0, h->stream>>>(L, R, h->g, a, S, c);
+      else if (bc == 1) wave<Links64T<true>, 1, KIND_METRO><<<grid, kBlock, 0, h->stream>>>(L, R, h->g, a, S, c);
+      else wave<Links64T<true>, 2, KIND_METRO><<<grid, kBlock, 0, h->stream>>>(L, R, h->g, a, S, c);
+    }
+  } else {
+    Links32T<true> L{h->q32, h->g.vh};
+    if (sk == KIND_HB) {
+      if (bc == 0) wave<Links32T<true>, 0, KIND_HB><<<grid, kBlock, 0, h->stream>>>(L, R, h->g, a, S, c);
+      else if (bc == 1) wave<Links32T<true>, 1, KIND_HB><<<grid, kBlock, 0, h->stream>>>(L, R, h->g, a, S, c);
+      else wave<Links32T<true>, 2, KIND_HB><<<grid, kBlock, 0, h->stream>>>(L, R, h->g, a, S, c);
+    } else {
+      if (bc == 0) wave<Links32T<true>, 0, KIND_METRO><<<grid, kBlock, 0, h->stream>>>(L, R, h->g, a, S, c);
+      else if (bc == 1) wave<Links32T<true>, 1, KIND_METRO><<<grid, kBlock, 0, h->stream>>>(L, R, h->g, a, S, c);
+      else wave<Links32T<true>, 2, KIND_METRO><<<grid, kBlock, 0, h->stream>>>(L, R, h->g, a, S, c);
+    }
+  }
+  LAUNCH_CHECK(h);
+  for (int i = 0; i < np; i++)
+    if (ps[i].kind != KIND_METRO) h->unit_passes++;
+  return QCD_OK;
+}
+
+bool use_wave(const qcd_lattice* h) {
+  if (h->sched == QCD_SCHED_WAVEFRONT) return true;
+  if (h->sched == QCD_SCHED_PHASES) return false;
+  // automatic: per-phase launches (measured faster on B200 at every size so
+  // far); the wavefront is selected explicitly
+  return false;
+}
+
+int run_passes(qcd_lattice* h, const PassSpec* ps, int np);
+
 int check_device_error(qcd_lattice* h) {
   int e = 0;
   CUDA_OR_FAIL(h, cudaMemcpyAsync(&h->result_host[2], h->err, sizeof(int), cudaMemcpyDeviceToHost,
                                   h->stream));
   CUDA_OR_FAIL(h, cudaStreamSynchronize(h->stream));
   memcpy(&e, &h->result_host[2], sizeof(int));
+  if (e & DEVERR_TIMEOUT) {
+    CUDA_OR_FAIL(h, cudaMemsetAsync(h->err, 0, sizeof(int), h->stream));
+    CUDA_OR_FAIL(h, cudaStreamSynchronize(h->stream));
+    return fail(h, QCD_ERR_TIMEOUT, "a wavefront task waited longer than its bound for a neighbour slice");
+  }
   if (e & DEVERR_HB_LOOP)
     return fail(h, QCD_ERR_NONUNITARY,
                 "heat-bath rejection loop exceeded %d tries (staple sum zero or not finite)",
@@ -191,6 +472,25 @@ int launch_measure(qcd_lattice* h, double* out_dev) {
   return QCD_OK;
 }
 
+int run_passes(qcd_lattice* h, const PassSpec* ps, int np) {
+  if (np == 0) return QCD_OK;
+  if (use_wave(h)) {
+    int rc = wave_setup(h);
+    if (rc) return rc;
+    for (int i = 0; i < np; i += h->wave_chain) {
+      const int k = np - i < h->wave_chain ? np - i : h->wave_chain;
+      rc = launch_wave(h, ps + i, k);
+      if (rc) return rc;
+    }
+    return QCD_OK;
+  }
+  for (int i = 0; i < np; i++) {
+    int rc = pass(h, ps[i].kind, ps[i].renorm);
+    if (rc) return rc;
+  }
+  return QCD_OK;
+}
+
 void release(qcd_lattice* h) {
   cudaFree(h->lo);
   cudaFree(h->hi);
@@ -203,6 +503,10 @@ void release(qcd_lattice* h) {
   cudaFree(h->err);
   cudaFree(h->series);
   cudaFree(h->aos_stage);
+  cudaFree(h->wave_done);
+  cudaFree(h->wave_queue);
+  cudaFree(h->wave_abort);
+  for (int i = 0; i < 5; i++) cudaFree(h->wave_tasks[i]);
   if (h->result_host) cudaFreeHost(h->result_host);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
 }
@@ -409,31 +713,87 @@ int qcd_normalize(qcd_lattice* h) {
 int qcd_sweep(qcd_lattice* h, int n) {
   if (!h || n < 0) return QCD_ERR_INVALID;
   const int kind = h->p.algo == QCD_ALGO_HEATBATH ? KIND_HB : KIND_METRO;
+  PassSpec buf[64];
+  int np = 0;
   for (int i = 0; i < n; i++) {
     const bool renorm = h->p.renorm_every > 0 && (h->sweeps_done + 1) % h->p.renorm_every == 0;
     // FP32: the re-projection rides on the sweep's last pass, each link being
     // re-projected at its last update (no extra read of the store); FP64
     // keeps the reference's separate normalize after the sweep
     const bool fused = renorm && h->p.precision == QCD_PREC_FP32;
-    int rc = pass(h, kind, fused && h->p.n_or == 0);
-    for (int r = 0; rc == QCD_OK && r < h->p.n_or; r++) rc = pass(h, KIND_OR, fused && r == h->p.n_or - 1);
-    if (rc) return rc;
+    if (np + 1 + h->p.n_or > 64) {
+      int rc = run_passes(h, buf, np);
+      if (rc) return rc;
+      np = 0;
+    }
+    buf[np++] = PassSpec{kind, fused && h->p.n_or == 0};
+    for (int r = 0; r < h->p.n_or; r++) buf[np++] = PassSpec{KIND_OR, fused && r == h->p.n_or - 1};
     h->sweeps_done++;
     if (renorm && !fused) {
-      rc = qcd_normalize(h);
+      int rc = run_passes(h, buf, np);
+      np = 0;
+      if (rc == QCD_OK) rc = qcd_normalize(h);
       if (rc) return rc;
     }
   }
-  return QCD_OK;
+  return run_passes(h, buf, np);
 }
 
 int qcd_overrelax(qcd_lattice* h, int n) {
   if (!h || n < 0) return QCD_ERR_INVALID;
-  for (int i = 0; i < n; i++) {
-    int rc = pass(h, KIND_OR);
+  PassSpec buf[64];
+  while (n > 0) {
+    const int k = n < 64 ? n : 64;
+    for (int i = 0; i < k; i++) buf[i] = PassSpec{KIND_OR, 0};
+    int rc = run_passes(h, buf, k);
     if (rc) return rc;
+    n -= k;
   }
   return QCD_OK;
+}
+
+int qcd_set_schedule(qcd_lattice* h, int mode) {
+  if (!h || mode < QCD_SCHED_AUTO || mode > QCD_SCHED_WAVEFRONT) return QCD_ERR_INVALID;
+  h->sched = mode;
+  return QCD_OK;
+}
+
+int qcd_get_schedule(const qcd_lattice* h) {
+  if (!h) return QCD_ERR_INVALID;
+  return use_wave(h) ? QCD_SCHED_WAVEFRONT : QCD_SCHED_PHASES;
+}
+
+int qcd_set_wave_tuning(qcd_lattice* h, int chunk_sites, int passes_per_launch, int fronts) {
+  if (!h || chunk_sites < 0 || passes_per_launch < 0 || passes_per_launch > kMaxWavePhases / 6 || fronts < 0)
+    return QCD_ERR_INVALID;
+  if (fronts && (h->g.lt % fronts || h->g.lt / fronts < 2))
+    return fail(h, QCD_ERR_INVALID, "fronts must divide Lt = %d into arcs of >= 2 slices", h->g.lt);
+  int rc = wave_setup(h);
+  if (rc) return rc;
+  if (chunk_sites) h->wave_chunk = (chunk_sites + kBlock - 1) / kBlock * kBlock;
+  if (passes_per_launch) h->wave_chain = passes_per_launch;
+  if (fronts) h->wave_fronts = fronts;
+  return QCD_OK;
+}
+
+int qcd_wave_plan(const int* mu, const int* par, int n_phases, int* seam, int* start, int* need) {
+  if (!mu || !par || !seam || !start || !need || n_phases < 1 || n_phases > kMaxWavePhases)
+    return QCD_ERR_INVALID;
+  short nd[3][kMaxWavePhases];
+  int rc = plan_wave(mu, par, n_phases, nd, seam, start);
+  if (rc) return rc;
+  for (int o = 0; o < 3; o++)
+    for (int n = 0; n < n_phases; n++) need[o * n_phases + n] = nd[o][n];
+  return QCD_OK;
+}
+
+int qcd_wave_selftest_timeout(qcd_lattice* h) {
+  if (!h) return QCD_ERR_INVALID;
+  PassSpec p{KIND_OR, 0};
+  int rc = launch_wave(h, &p, 1, /*stall_test=*/1, /*spin=*/4096);
+  if (rc) return rc;
+  h->unit_passes--;  // the pass did not complete
+  return check_device_error(h);
 }
 
 int qcd_measure(qcd_lattice* h, double* energy, double* plaquette) {

@@ -14,30 +14,43 @@
 
 namespace qcd {
 
-struct RngStore {
+template <bool CG>
+struct RngStoreT {
   uint32_t* w;  // w[j * vh + id], j = 0..2 -> s1[j], j = 3..5 -> s2[j-3]
   int vh;
 
+  __device__ __forceinline__ uint32_t get(int j, int id) const {
+    const uint32_t* p = w + (size_t)j * vh + id;
+    return CG ? __ldcg(p) : *p;
+  }
+  __device__ __forceinline__ void put(int j, int id, uint32_t v) const {
+    uint32_t* p = w + (size_t)j * vh + id;
+    if (CG)
+      __stcg(p, v);
+    else
+      *p = v;
+  }
   __device__ __forceinline__ void load(int id, curandStateMRG32k3a_t* s) const {
-    s->s1[0] = w[0 * (size_t)vh + id];
-    s->s1[1] = w[1 * (size_t)vh + id];
-    s->s1[2] = w[2 * (size_t)vh + id];
-    s->s2[0] = w[3 * (size_t)vh + id];
-    s->s2[1] = w[4 * (size_t)vh + id];
-    s->s2[2] = w[5 * (size_t)vh + id];
+    s->s1[0] = get(0, id);
+    s->s1[1] = get(1, id);
+    s->s1[2] = get(2, id);
+    s->s2[0] = get(3, id);
+    s->s2[1] = get(4, id);
+    s->s2[2] = get(5, id);
     s->boxmuller_flag = 0;
     s->boxmuller_flag_double = 0;
     s->boxmuller_extra = 0.f;
     s->boxmuller_extra_double = 0.0;
   }
   __device__ __forceinline__ void store(int id, const curandStateMRG32k3a_t* s) const {
-    w[0 * (size_t)vh + id] = s->s1[0];
-    w[1 * (size_t)vh + id] = s->s1[1];
-    w[2 * (size_t)vh + id] = s->s1[2];
-    w[3 * (size_t)vh + id] = s->s2[0];
-    w[4 * (size_t)vh + id] = s->s2[1];
-    w[5 * (size_t)vh + id] = s->s2[2];
+    put(0, id, s->s1[0]);
+    put(1, id, s->s1[1]);
+    put(2, id, s->s1[2]);
+    put(3, id, s->s2[0]);
+    put(4, id, s->s2[1]);
+    put(5, id, s->s2[2]);
   }
 };
+typedef RngStoreT<false> RngStore;
 
 }  // namespace qcd
