@@ -192,6 +192,20 @@ const char* qcd_last_error(const qcd_lattice* h);
 const char* qcd_status_string(int status);
 
 /* ------------------------------------------------------------------------
+ * Statistics of a measurement series (host only, no GPU).
+ * The reference's naive mean / population variance and normalised
+ * autocorrelation of lags 1..w (mean_variance, autocorrelation,
+ * statistics.h:30-51), and what its README leaves to post-processing
+ * (README.md:74): the binned error of the mean and the integrated
+ * autocorrelation time tau_int = 1/2 + sum_{t<=W} rho(t) with the
+ * Madras-Sokal window (smallest W >= c tau_int(W)) and its error.
+ * ------------------------------------------------------------------------ */
+int qcd_stats_mean_variance(const double* x, int n, double* mean, double* var);
+int qcd_stats_autocorrelation(const double* x, int n, int w, double mean, double var, double* out);
+int qcd_stats_binned(const double* x, int n, int bin, double* mean, double* err);
+int qcd_stats_tau_int(const double* x, int n, double c, double* tau, int* window, double* dtau);
+
+/* ------------------------------------------------------------------------
  * Random-number tape.  For stream id in [first, first+n_streams), seeded as
  * curand_init(seed, id, 0) exactly like setup_kernel (lattice_setup.h:15-21),
  * record the first n_draws draws.  Draw k is taken both as curand_uniform

@@ -30,6 +30,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <math.h>
+#include <time.h>
 #include <vector>
 #include <string>
 #include <cuda_runtime.h>
@@ -47,6 +48,8 @@ namespace ref_hb {
 #include "mc_updates_pcc.h"
 #include "mc_updates_pmc.h"
 #include "observables.h"
+#include "statistics.h"
+#include "output.h"
 #undef ALGO
 }  // namespace ref_hb
 
@@ -58,6 +61,8 @@ namespace ref_metro {
 #include "mc_updates_pcc.h"
 #include "mc_updates_pmc.h"
 #include "observables.h"
+#include "statistics.h"
+#include "output.h"
 #undef ALGO
 }  // namespace ref_metro
 
@@ -130,6 +135,10 @@ struct Args {
   std::string out = "ref";
   long long first = 0;
   int n_streams = 0, n_draws = 0;
+  // knobs of kernel.cu's main (mode "main")
+  int readconf = 0, sconf = 0, save = 0, N = 100, N_term = 10, N_block = 20, Nblock_term = 10, Nsave = 5,
+      N_cor = 1, W = 10;
+  std::string nsave = "1", nconfr = "1", nconfs = "1";
 };
 
 static void usage() {
@@ -137,7 +146,8 @@ static void usage() {
           "ref_harness tape|run|bench [--lt N --lx N --ly N --beta B --eps E "
           "--upd U --algo hb|metro|or --bc 0|1|2 --hot 0|1 --seed S --sweeps K "
           "--warmup W --dumps a,b,c --phase-dumps 0|1 --measure 0|1 --out PREFIX "
-          "--first F --streams N --draws D]\n");
+          "--first F --streams N --draws D] [main: --readconf --sconf --save --N --N-term --N-block "
+          "--Nblock-term --Nsave --N-cor --W --nsave --nconfr --nconfs]\n");
   exit(2);
 }
 
@@ -179,6 +189,19 @@ static Args parse(int argc, char** argv) {
     else if (k == "--first") a.first = atoll(v);
     else if (k == "--streams") a.n_streams = atoi(v);
     else if (k == "--draws") a.n_draws = atoi(v);
+    else if (k == "--readconf") a.readconf = atoi(v);
+    else if (k == "--sconf") a.sconf = atoi(v);
+    else if (k == "--save") a.save = atoi(v);
+    else if (k == "--N") a.N = atoi(v);
+    else if (k == "--N-term") a.N_term = atoi(v);
+    else if (k == "--N-block") a.N_block = atoi(v);
+    else if (k == "--Nblock-term") a.Nblock_term = atoi(v);
+    else if (k == "--Nsave") a.Nsave = atoi(v);
+    else if (k == "--N-cor") a.N_cor = atoi(v);
+    else if (k == "--W") a.W = atoi(v);
+    else if (k == "--nsave") a.nsave = v;
+    else if (k == "--nconfr") a.nconfr = v;
+    else if (k == "--nconfs") a.nconfs = v;
     else usage();
   }
   return a;
@@ -362,6 +385,162 @@ static void write_file(const std::string& name, const void* p, size_t bytes) {
 DEFINE_DRIVER(ref_hb)
 DEFINE_DRIVER(ref_metro)
 
+// kernel.cu:49-268 with the knobs at run time: the same calls, in the same
+// order, to the reference's own functions (setup, starts, mc_up_*, normalize,
+// en_av, mean_variance, autocorrelation, mean_lattice, save_*, read_conf,
+// save_conf, print_det); output files land in the working directory.
+#define DEFINE_MAIN(NS)                                                                      \
+  static int NS##_kernel_main(const Args& a) {                                               \
+    char nsave[16], nconfr[16], nconfs[16];                                                   \
+    snprintf(nsave, sizeof nsave, "%s", a.nsave.c_str());                                     \
+    snprintf(nconfr, sizeof nconfr, "%s", a.nconfr.c_str());                                  \
+    snprintf(nconfs, sizeof nconfs, "%s", a.nconfs.c_str());                                  \
+    int Nterms = 0, inits;                                                                    \
+    NS::lattice l = {a.ly, a.lx, a.lt, a.ly * a.lx * a.lt, 3, 4, 12, (float)a.beta,           \
+                     (float)a.eps, a.upd};                                                    \
+    NS::lattice l2 = {l.y / 2, l.x, l.t, l.V / 2, 3, 4, 12, l.beta, l.epsilon, a.upd};        \
+    printf("N %d Lt %d L %d Ly %d V %d Dim %d DimRep %d Dimtot %d \n", a.N, l.t, l.x, l.y,    \
+           l.V, l.d, l.dg, l.dt);                                                             \
+    if (l.t % 2 || l.x % 2 || l.y % 2) {                                                      \
+      printf("Lt, Lx and Ly must be even\n");                                                 \
+      return 1;                                                                               \
+    }                                                                                         \
+    int nblocks, nthreads = 256;                                                              \
+    while (l2.V % nthreads != 0) nthreads--;                                                  \
+    nblocks = 2 * (l2.V / nthreads);                                                          \
+    printf("nblocks %d nthreads %d\n", nblocks, nthreads);                                    \
+    if (a.algo == METROPOLIS)                                                                 \
+      printf("METROPOLIS UPDATES epsilon %.2f hits %d\n", l.epsilon, l.updates);              \
+    if (a.algo == HEATBATH) printf("HEAT-BATH UPDATES\n");                                    \
+    int hits = (a.algo == METROPOLIS) ? l.updates : 1;                                        \
+    curandStateMRG32k3a_t* devStates;                                                         \
+    CK(cudaMalloc((void**)&devStates, l2.V * sizeof(curandStateMRG32k3a_t)));                 \
+    NS::setup_kernel<<<nblocks / 2, nthreads>>>(devStates, (int)a.seed);                      \
+    double *phi = (double*)malloc(l.V * l.dt * sizeof(double)), *phid;                        \
+    CK(cudaMalloc(&phid, l.V * l.dt * sizeof(double)));                                       \
+    char bound[12];                                                                           \
+    snprintf(bound, sizeof bound, "%s", a.bc == 0 ? "per" : a.bc == 1 ? "pcc" : "pmc");       \
+    if (a.bc == 0) printf("PERIODIC BOUNDARY CONDITIONS\n\n");                                \
+    else if (a.bc == 1) printf("PERFECT COLOUR CONDUCTOR BOUNDARY CONDITIONS\n\n");           \
+    else printf("PERFECT MAGNETIC CONDUCTOR BOUNDARY CONDITIONS\n\n");                         \
+    if (a.readconf == 0) {                                                                    \
+      inits = a.hot ? 0 : 1;                                                                  \
+      if (a.hot) {                                                                            \
+        if (a.bc == 1) NS::rand_init2_pcc<<<nblocks / 2, nthreads>>>(phid, devStates, l2);    \
+        else NS::rand_init2<<<nblocks / 2, nthreads>>>(phid, devStates, l2);                  \
+      } else {                                                                                \
+        NS::id_init2<<<nblocks / 2, nthreads>>>(phid, l2);                                    \
+      }                                                                                       \
+    } else {                                                                                  \
+      NS::read_conf(phi, l, &Nterms, &inits, bound, nconfr);                                  \
+      CK(cudaMemcpy(phid, phi, l.V * l.dt * sizeof(double), cudaMemcpyHostToDevice));         \
+    }                                                                                         \
+    CK(cudaMemcpy(phi, phid, l.V * l.dt * sizeof(double), cudaMemcpyDeviceToHost));           \
+    NS::print_det(phi, l);                                                                    \
+    int *accept, *accepth = (int*)malloc(l.V * sizeof(int));                                  \
+    CK(cudaMalloc(&accept, l.V * sizeof(int)));                                               \
+    CK(cudaMemset(accept, 0, l.V * sizeof(int)));                                             \
+    double *end, *en = (double*)malloc(a.N * sizeof(double));                                 \
+    CK(cudaMalloc(&end, a.N * sizeof(double)));                                               \
+    CK(cudaMemset(end, 0, a.N * sizeof(double)));                                             \
+    double *end2, *en2 = (double*)malloc(a.N * sizeof(double));                               \
+    CK(cudaMalloc(&end2, a.N * sizeof(double)));                                              \
+    CK(cudaMemset(end2, 0, a.N * sizeof(double)));                                            \
+    int i, j;                                                                                 \
+    int t_ini, t_ini_mc, t_fin, t_n, block_size_t = a.N_term / a.Nblock_term,                 \
+        block_size = a.N / a.N_block, block_s_size = a.N / a.Nsave;                           \
+    t_ini = time(NULL);                                                                       \
+    t_n = time(NULL);                                                                         \
+    double energy[2], energy2[2];                                                             \
+    std::vector<double> autoc(a.W), autoc2(a.W);                                              \
+    double saccept;                                                                           \
+    if (a.readconf < 2) {                                                                     \
+      for (i = 1; i < a.N_term + 1; i++) {                                                    \
+        if (i % 100 == 0) NS::normalize<<<nblocks, nthreads>>>(phid, l);                      \
+        NS##_sweep(a.bc, 0, nblocks, nthreads, phid, devStates, accept, l2);                  \
+        if (block_size_t > 0 && i % block_size_t == 0) {                                      \
+          printf("%lf Time %d Left(min)%lf\n", (double)i / (a.N_term), (int)(time(NULL) - t_n), \
+                 (double)(time(NULL) - t_ini) * (a.N_term - i) / i / 60);                     \
+          fflush(stdout);                                                                     \
+          t_n = time(NULL);                                                                   \
+        }                                                                                     \
+      }                                                                                       \
+      NS::normalize<<<nblocks, nthreads>>>(phid, l);                                          \
+      Nterms = a.N_term + Nterms;                                                             \
+      if (a.sconf == 0) {                                                                     \
+        CK(cudaMemcpy(phi, phid, l.V * l.dt * sizeof(double), cudaMemcpyDeviceToHost));       \
+        NS::save_conf(phi, l, Nterms, inits, bound, nconfs);                                  \
+      }                                                                                       \
+    }                                                                                         \
+    CK(cudaMemcpy(phi, phid, l.V * l.dt * sizeof(double), cudaMemcpyDeviceToHost));           \
+    NS::print_det(phi, l);                                                                    \
+    CK(cudaMemset(accept, 0, l.V * sizeof(int)));                                             \
+    t_ini_mc = time(NULL);                                                                    \
+    t_n = time(NULL);                                                                         \
+    for (i = 1; i < a.N + 1; i++) {                                                           \
+      for (j = 0; j < a.N_cor; j++) NS##_sweep(a.bc, 0, nblocks, nthreads, phid, devStates, accept, l2); \
+      if (i % 100 == 0) NS::normalize<<<nblocks, nthreads>>>(phid, l);                        \
+      if (a.bc == 2) NS::en_av<1><<<nblocks, nthreads>>>(phid, end + i - 1, end2 + i - 1, l2); \
+      else NS::en_av<0><<<nblocks, nthreads>>>(phid, end + i - 1, end2 + i - 1, l2);          \
+      if (block_size > 0 && i % block_size == 0) {                                            \
+        printf("%lf Time %d Left(min)%lf\n", (double)i / a.N, (int)(time(NULL) - t_n),       \
+               (double)(time(NULL) - t_ini_mc) * (a.N - i) / i / 60);                         \
+        t_n = time(NULL);                                                                     \
+        fflush(stdout);                                                                       \
+      }                                                                                       \
+      if (block_s_size > 0 && i % block_s_size == 0) {                                        \
+        CK(cudaMemcpy(en, end, i * sizeof(double), cudaMemcpyDeviceToHost));                  \
+        CK(cudaMemcpy(en2, end2, i * sizeof(double), cudaMemcpyDeviceToHost));                \
+        printf("Energy ");                                                                    \
+        NS::mean_variance(en, i, energy, true);                                               \
+        NS::autocorrelation(en, i, a.W, energy[0], energy[1], autoc.data());                  \
+        printf("Plaquette ");                                                                 \
+        NS::mean_variance(en2, i, energy2, true);                                             \
+        NS::autocorrelation(en2, i, a.W, energy2[0], energy2[1], autoc2.data());              \
+        fflush(stdout);                                                                       \
+        if (a.save == 0) {                                                                    \
+          saccept = NS::mean_lattice(accept, accepth, i * a.N_cor * l.d * hits, l, false);    \
+          if (a.bc == 1) saccept = saccept / ((double)(l.y - 1) / l.y + 1 / (double)l.y / 3); \
+          NS::save_energy(energy[0], energy[1], Nterms, a.N, a.N_cor, saccept, l, bound, nsave); \
+          NS::save_energy_av(energy[0], energy[1], energy2[0], energy2[1], Nterms, a.N, a.N_cor, \
+                             saccept, l, bound, nsave);                                       \
+          NS::save_autocorrelation(autoc.data(), a.W, i, a.N_cor, Nterms, l, bound, nsave);   \
+          NS::save_autocorrelation_av(autoc2.data(), a.W, i, a.N_cor, Nterms, l, bound, nsave); \
+          NS::save_en_seq(en2, en, Nterms, i, a.N_cor, 1, l, bound, nsave);                   \
+        }                                                                                     \
+      }                                                                                       \
+    }                                                                                         \
+    t_fin = time(NULL);                                                                       \
+    printf("Time %d\n", t_fin - t_ini);                                                       \
+    CK(cudaMemcpy(en, end, a.N * sizeof(double), cudaMemcpyDeviceToHost));                    \
+    CK(cudaMemcpy(en2, end2, a.N * sizeof(double), cudaMemcpyDeviceToHost));                  \
+    saccept = NS::mean_lattice(accept, accepth, a.N * a.N_cor * l.d * hits, l, true);         \
+    if (a.bc == 1) saccept = saccept / ((double)(l.y - 1) / l.y + 1 / (double)l.y / 3);       \
+    printf("accept %lf\n\n", saccept);                                                        \
+    printf("Energy ");                                                                        \
+    NS::mean_variance(en, a.N, energy, true);                                                 \
+    NS::autocorrelation(en, a.N, a.W, energy[0], energy[1], autoc.data());                    \
+    printf("Plaquette ");                                                                     \
+    NS::mean_variance(en2, a.N, energy2, true);                                               \
+    NS::autocorrelation(en2, a.N, a.W, energy2[0], energy2[1], autoc2.data());                \
+    if (a.save == 0) {                                                                        \
+      NS::save_energy(energy[0], energy[1], Nterms, a.N, a.N_cor, saccept, l, bound, nsave);  \
+      NS::save_energy_av(energy[0], energy[1], energy2[0], energy2[1], Nterms, a.N, a.N_cor,  \
+                         saccept, l, bound, nsave);                                           \
+      NS::save_en_seq(en2, en, Nterms, a.N, a.N_cor, 1, l, bound, nsave);                     \
+      NS::save_autocorrelation(autoc.data(), a.W, a.N, a.N_cor, Nterms, l, bound, nsave);     \
+      NS::save_autocorrelation_av(autoc2.data(), a.W, a.N, a.N_cor, Nterms, l, bound, nsave); \
+    }                                                                                         \
+    CK(cudaGetLastError());                                                                   \
+    free(phi); free(accepth); cudaFree(phid); cudaFree(accept); cudaFree(devStates);          \
+    free(en); free(en2); cudaFree(end); cudaFree(end2);                                       \
+    return 0;                                                                                 \
+  }
+
+DEFINE_MAIN(ref_hb)
+DEFINE_MAIN(ref_metro)
+
+
 int main(int argc, char** argv) {
   Args a = parse(argc, argv);
   if (a.mode == "tape") {
@@ -382,6 +561,7 @@ int main(int argc, char** argv) {
     cudaFree(d);
     return 0;
   }
+  if (a.mode == "main") return a.algo == METROPOLIS ? ref_metro_kernel_main(a) : ref_hb_kernel_main(a);
   if (a.mode != "run" && a.mode != "bench") usage();
   // over-relaxation (update==1) and heat-bath share the HEATBATH namespace: the
   // `update` flag bypasses link_update (mc_updates.h:178-181).

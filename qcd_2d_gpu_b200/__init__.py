@@ -129,6 +129,10 @@ _SIGS = {
     "qcd_wave_plan": (_I, [_P, _P, _I, _P, _P, _P]),
     "qcd_wave_selftest_timeout": (_I, [_P]),
     "qcd_set_wave_tuning": (_I, [_P, _I, _I, _I]),
+    "qcd_stats_mean_variance": (_I, [_P, _I, _DP, _DP]),
+    "qcd_stats_autocorrelation": (_I, [_P, _I, _I, _D, _D, _P]),
+    "qcd_stats_binned": (_I, [_P, _I, _I, _DP, _DP]),
+    "qcd_stats_tau_int": (_I, [_P, _I, _D, _DP, ctypes.POINTER(ctypes.c_int), _DP]),
 }
 
 
@@ -333,3 +337,48 @@ def wave_plan(mu, par, lib: ctypes.CDLL | None = None):
     if rc != QCD_OK:
         raise QcdError(rc, "qcd_wave_plan")
     return seam, start, need.reshape(3, n)
+
+
+# -- statistics of measurement series (host code of the library) ------------
+def _series(x):
+    return np.ascontiguousarray(x, dtype=np.float64)
+
+
+def mean_variance(x):
+    """The reference's naive mean and population variance (statistics.h:30-39)."""
+    lib = load_library()
+    a = _series(x)
+    m, v = ctypes.c_double(), ctypes.c_double()
+    if lib.qcd_stats_mean_variance(_ptr(a), len(a), ctypes.byref(m), ctypes.byref(v)):
+        raise QcdError(-1, "mean_variance")
+    return m.value, v.value
+
+
+def autocorrelation(x, w, mean, var):
+    """The reference's normalised autocorrelation of lags 1..w (statistics.h:41-51)."""
+    lib = load_library()
+    a = _series(x)
+    out = np.zeros(w)
+    if lib.qcd_stats_autocorrelation(_ptr(a), len(a), w, mean, var, _ptr(out)):
+        raise QcdError(-1, "autocorrelation")
+    return out
+
+
+def binned(x, bin_size):
+    lib = load_library()
+    a = _series(x)
+    m, e = ctypes.c_double(), ctypes.c_double()
+    if lib.qcd_stats_binned(_ptr(a), len(a), bin_size, ctypes.byref(m), ctypes.byref(e)):
+        raise QcdError(-1, "binned")
+    return m.value, e.value
+
+
+def tau_int(x, c=6.0):
+    """Integrated autocorrelation time, Madras-Sokal window: (tau, W, dtau)."""
+    lib = load_library()
+    a = _series(x)
+    t, d = ctypes.c_double(), ctypes.c_double()
+    w = ctypes.c_int()
+    if lib.qcd_stats_tau_int(_ptr(a), len(a), c, ctypes.byref(t), ctypes.byref(w), ctypes.byref(d)):
+        raise QcdError(-1, "tau_int")
+    return t.value, w.value, d.value

@@ -12,6 +12,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libqcd2d.so")
+DRIVER = os.path.join(HERE, "qcd2d")
+DRIVER_SRC = [os.path.join(HERE, "driver", f) for f in ("qcd2d_main.c", "refio.c")]
 
 NVCC_FLAGS = [
     "-O3",
@@ -26,7 +28,7 @@ NVCC_FLAGS = [
 
 
 def sources() -> list[str]:
-    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cu", ".cuh"))]
+    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cu", ".cuh", ".cc"))]
 
 
 def needs_build() -> bool:
@@ -47,6 +49,7 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
         "-o",
         LIB + ".tmp",
         os.path.join(CSRC, "qcd2d.cu"),
+        os.path.join(CSRC, "stats.cc"),
     ]
     if verbose:
         print(" ".join(cmd), flush=True)
@@ -55,6 +58,23 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+def build_driver(force: bool = False, verbose: bool = False) -> str:
+    """The drop-in program (C), linked against the in-tree libqcd2d.so."""
+    build_library(verbose=verbose)
+    deps = DRIVER_SRC + [os.path.join(HERE, "driver", "refio.h"), os.path.join(ROOT, "include", "qcd2d.h"), LIB]
+    if not force and os.path.exists(DRIVER) and all(os.path.getmtime(d) <= os.path.getmtime(DRIVER) for d in deps):
+        return DRIVER
+    cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
+    cmd = [cc, "-O2", "-std=gnu11", "-Wall", "-I" + os.path.join(ROOT, "include"), "-o", DRIVER + ".tmp"] + DRIVER_SRC + [
+        "-L" + HERE, "-lqcd2d", "-Wl,-rpath,$ORIGIN", "-lm"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(DRIVER + ".tmp", DRIVER)
+    return DRIVER
+
+
 if __name__ == "__main__":
     build_library(force="--force" in sys.argv, verbose=True)
+    build_driver(force="--force" in sys.argv, verbose=True)
     print(LIB)
