@@ -192,6 +192,50 @@ const char* qcd_last_error(const qcd_lattice* h);
 const char* qcd_status_string(int status);
 
 /* ------------------------------------------------------------------------
+ * Batched replicas (no counterpart in the reference, which runs one lattice
+ * per process).  Many independent lattices of different size, coupling,
+ * boundary condition and start share one set of launches: a sweep of the
+ * whole batch is the six phase launches of one lattice, each covering every
+ * replica, and a measurement is one launch writing every replica's
+ * (energy, plaquette).  qcd_batch_run captures one measurement interval as a
+ * CUDA graph and replays it.  Replica r draws from MRG32k3a streams
+ * curand_init(seed_r, stream_offset_r + id, 0): with stream_offset 0 it
+ * reproduces a single lattice of the same seed; giving replicas disjoint
+ * offset blocks under one seed keeps every stream of the batch distinct.
+ * ------------------------------------------------------------------------ */
+typedef struct qcd_replica {
+  int lt, lx, ly;          /* even extents */
+  float beta;
+  int boundary;            /* enum qcd_boundary */
+  int hot;                 /* 1: hot start (rand_init2 / rand_init2_pcc), 0: cold */
+  unsigned long long seed;
+  long long stream_offset; /* first MRG32k3a subsequence of this replica */
+} qcd_replica;
+typedef struct qcd_batch qcd_batch;
+
+/* common: algo, precision, epsilon, upd, n_or, renorm_every apply to every
+   replica (its extents, beta, boundary and seed are ignored) */
+int qcd_batch_create(const qcd_replica* replicas, int n, const qcd_params* common, qcd_batch** out);
+int qcd_batch_destroy(qcd_batch* b);
+int qcd_batch_set_stream(qcd_batch* b, void* stream);
+/* seed every replica's streams and apply its start */
+int qcd_batch_init(qcd_batch* b);
+/* room for `capacity` measurements per replica (resets the series) */
+int qcd_batch_reserve(qcd_batch* b, int capacity);
+/* `sweeps` sweeps of every replica, measuring after every `measure_every`
+   sweeps (0: never); with use_graph the interval runs as a CUDA graph */
+int qcd_batch_run(qcd_batch* b, int sweeps, int measure_every, int use_graph);
+/* wait for the batch's stream; reports device-side errors */
+int qcd_batch_synchronize(qcd_batch* b);
+/* measurements taken so far (per replica) */
+int qcd_batch_measured(qcd_batch* b);
+int qcd_batch_series(qcd_batch* b, int replica, double* energy, double* plaquette, int n);
+/* replica's configuration in the reference's AoS FP64 layout */
+int qcd_batch_store_config(qcd_batch* b, int replica, double* aos_host);
+long long qcd_batch_sites(const qcd_batch* b);
+const char* qcd_batch_last_error(const qcd_batch* b);
+
+/* ------------------------------------------------------------------------
  * Statistics of a measurement series (host only, no GPU).
  * The reference's naive mean / population variance and normalised
  * autocorrelation of lags 1..w (mean_variance, autocorrelation,

@@ -76,6 +76,21 @@ class Params(ctypes.Structure):
     ]
 
 
+class Replica(ctypes.Structure):
+    """qcd_replica (include/qcd2d.h)."""
+
+    _fields_ = [
+        ("lt", ctypes.c_int),
+        ("lx", ctypes.c_int),
+        ("ly", ctypes.c_int),
+        ("beta", ctypes.c_float),
+        ("boundary", ctypes.c_int),
+        ("hot", ctypes.c_int),
+        ("seed", ctypes.c_ulonglong),
+        ("stream_offset", ctypes.c_longlong),
+    ]
+
+
 TAPE_DTYPE = np.dtype(
     [
         ("ud", "<f8"),
@@ -129,6 +144,18 @@ _SIGS = {
     "qcd_wave_plan": (_I, [_P, _P, _I, _P, _P, _P]),
     "qcd_wave_selftest_timeout": (_I, [_P]),
     "qcd_set_wave_tuning": (_I, [_P, _I, _I, _I]),
+    "qcd_batch_create": (_I, [_P, _I, ctypes.POINTER(Params), ctypes.POINTER(_P)]),
+    "qcd_batch_destroy": (_I, [_P]),
+    "qcd_batch_set_stream": (_I, [_P, _P]),
+    "qcd_batch_init": (_I, [_P]),
+    "qcd_batch_reserve": (_I, [_P, _I]),
+    "qcd_batch_run": (_I, [_P, _I, _I, _I]),
+    "qcd_batch_synchronize": (_I, [_P]),
+    "qcd_batch_measured": (_I, [_P]),
+    "qcd_batch_series": (_I, [_P, _I, _P, _P, _I]),
+    "qcd_batch_store_config": (_I, [_P, _I, _P]),
+    "qcd_batch_sites": (ctypes.c_longlong, [_P]),
+    "qcd_batch_last_error": (ctypes.c_char_p, [_P]),
     "qcd_stats_mean_variance": (_I, [_P, _I, _DP, _DP]),
     "qcd_stats_autocorrelation": (_I, [_P, _I, _I, _D, _D, _P]),
     "qcd_stats_binned": (_I, [_P, _I, _I, _DP, _DP]),
@@ -312,6 +339,91 @@ class Lattice:
         n = ctypes.c_size_t()
         self._check(self._lib.qcd_link_store(self._h, ctypes.byref(p), ctypes.byref(n)), "link_store")
         return p.value or 0, n.value
+
+
+class Batch:
+    """Many replicas advanced by shared launches (a qcd_batch handle).
+
+    replicas: sequence of dicts with keys lt, lx, ly, beta, boundary, hot, seed,
+    stream_offset (defaults: periodic, cold, seed 1234, offset 0).
+    """
+
+    def __init__(self, replicas, *, algo="heatbath", precision="fp32", epsilon=0.1, upd=1, n_or=0,
+                 renorm_every=0, lib: ctypes.CDLL | None = None):
+        self._lib = lib or load_library()
+        arr = (Replica * len(replicas))()
+        for i, r in enumerate(replicas):
+            bc = r.get("boundary", PERIODIC)
+            arr[i] = Replica(r["lt"], r["lx"], r["ly"], r["beta"], _BC[bc] if isinstance(bc, str) else int(bc),
+                             int(r.get("hot", 0)), int(r.get("seed", 1234)), int(r.get("stream_offset", 0)))
+        p = Params()
+        self._lib.qcd_params_default(ctypes.byref(p), 2, 2, 2)
+        p.algo = _ALGO[algo] if isinstance(algo, str) else int(algo)
+        p.precision = _PREC[precision] if isinstance(precision, str) else int(precision)
+        p.epsilon = epsilon
+        p.upd = upd
+        p.n_or = n_or
+        p.renorm_every = renorm_every
+        h = ctypes.c_void_p()
+        rc = self._lib.qcd_batch_create(arr, len(replicas), ctypes.byref(p), ctypes.byref(h))
+        if rc != QCD_OK:
+            raise QcdError(rc, "qcd_batch_create")
+        self._h = h
+        self.replicas = [dict(r) for r in replicas]
+        self.n = len(replicas)
+
+    def _check(self, rc, what):
+        if rc != QCD_OK:
+            msg = self._lib.qcd_batch_last_error(self._h)
+            raise QcdError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.qcd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr):
+        self._check(self._lib.qcd_batch_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)), "set_stream")
+
+    def init(self):
+        self._check(self._lib.qcd_batch_init(self._h), "init")
+
+    def reserve(self, capacity):
+        self._check(self._lib.qcd_batch_reserve(self._h, capacity), "reserve")
+
+    def run(self, sweeps, measure_every=1, graph=True):
+        self._check(self._lib.qcd_batch_run(self._h, sweeps, measure_every, int(graph)), "run")
+
+    def synchronize(self):
+        self._check(self._lib.qcd_batch_synchronize(self._h), "synchronize")
+
+    def measured(self):
+        k = self._lib.qcd_batch_measured(self._h)
+        if k < 0:
+            self._check(k, "measured")
+        return k
+
+    def series(self, replica, n=None):
+        n = self.measured() if n is None else n
+        e, p = np.zeros(n), np.zeros(n)
+        self._check(self._lib.qcd_batch_series(self._h, replica, _ptr(e), _ptr(p), n), "series")
+        return e, p
+
+    def store_config(self, replica):
+        r = self.replicas[replica]
+        out = np.empty(r["lt"] * r["lx"] * r["ly"] * 12)
+        self._check(self._lib.qcd_batch_store_config(self._h, replica, _ptr(out)), "store_config")
+        return out
+
+    @property
+    def sites(self):
+        return self._lib.qcd_batch_sites(self._h)
 
 
 def rng_tape(seed: int, first: int, n_streams: int, n_draws: int, lib: ctypes.CDLL | None = None) -> np.ndarray:

@@ -49,6 +49,7 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
         "-o",
         LIB + ".tmp",
         os.path.join(CSRC, "qcd2d.cu"),
+        os.path.join(CSRC, "batch.cu"),
         os.path.join(CSRC, "stats.cc"),
     ]
     if verbose:

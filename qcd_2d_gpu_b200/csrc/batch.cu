@@ -1,0 +1,625 @@
+// Batched replicas: many independent lattices of different size, coupling
+// and boundary condition advanced together.
+//
+// All replicas live in one link store and one RNG store (each replica's
+// planes contiguous, offsets in a device replica table).  One launch per
+// checkerboard phase covers every replica: CTA c belongs to the replica whose
+// [cta_begin, cta_begin + ceil(V/2 / 256)) range holds c, so a sweep of the
+// whole batch is 6 launches (plus passes of over-relaxation) instead of
+// 6 x n_replicas, and a measurement is one launch writing every replica's
+// (energy, plaquette) into a device series at a device-side cursor.  The
+// sweep + measurement is captured once as a CUDA graph and replayed.  The
+// per-link code is the single-lattice code (site32 / site64), so replica r
+// reproduces a single lattice with the same seed and stream offset.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <new>
+#include <vector>
+
+#include "qcd2d.h"
+#include "sites.cuh"
+
+using namespace qcd;
+
+namespace {
+
+struct Replica {
+  Geo g;
+  float beta;
+  int bc;
+  int hot;
+  long long link_off;  // float4 units (FP32) or double2 units per lo/hi plane (FP64)
+  long long rng_off;   // u32 words
+  long long site_off;  // accept counters
+  int cta_begin;       // first CTA of this replica in a batched launch
+  unsigned long long seed;
+  long long stream_off;
+};
+
+struct BatchView {
+  const Replica* rep;
+  int n;
+  float4* q32;
+  double2* lo;
+  double2* hi;
+  uint32_t* rng;
+};
+
+__device__ __forceinline__ int replica_of(const BatchView& B, int cta) {
+  int lo = 0, hi = B.n - 1;
+  while (lo < hi) {  // last replica with cta_begin <= cta
+    int mid = (lo + hi + 1) >> 1;
+    if (B.rep[mid].cta_begin <= cta)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+struct BatchArgs {
+  float eps;
+  int upd;
+  int* err;
+  int* accept;
+  int renorm;
+};
+
+template <int MU, int PAR, int KIND, bool FP64>
+__global__ void __launch_bounds__(kBlock) batch_phase(BatchView B, BatchArgs a) {
+  const int r = replica_of(B, blockIdx.x);
+  const Replica& R = B.rep[r];
+  const int id = (blockIdx.x - R.cta_begin) * kBlock + threadIdx.x;
+  if (id >= R.g.vh) return;
+  const Nbr n = make_nbr(R.g, id, PAR);
+  PhaseArgs pa{R.beta, a.eps, a.upd, a.err, a.accept ? a.accept + R.site_off : nullptr, a.renorm};
+  RngStore RS{B.rng + R.rng_off, R.g.vh};
+  if (FP64) {
+    Links64 L{B.lo + R.link_off, B.hi + R.link_off, R.g.vh};
+    switch (R.bc) {
+      case BC_PER: site64<MU, PAR, BC_PER, KIND, false>(L, RS, R.g, pa, n); break;
+      case BC_PCC: site64<MU, PAR, BC_PCC, KIND, false>(L, RS, R.g, pa, n); break;
+      default: site64<MU, PAR, BC_PMC, KIND, false>(L, RS, R.g, pa, n); break;
+    }
+  } else {
+    Links32 L{B.q32 + R.link_off, R.g.vh};
+    switch (R.bc) {
+      case BC_PER: site32<MU, PAR, BC_PER, KIND, false>(L, RS, R.g, pa, n, a.renorm); break;
+      case BC_PCC: site32<MU, PAR, BC_PCC, KIND, false>(L, RS, R.g, pa, n, a.renorm); break;
+      default: site32<MU, PAR, BC_PMC, KIND, false>(L, RS, R.g, pa, n, a.renorm); break;
+    }
+  }
+}
+
+// curand_init(seed_r, stream_off_r + id, 0) per site of every replica, then
+// the replica's start (rand_init2 / rand_init2_pcc / id_init2 semantics)
+template <bool FP64>
+__global__ void __launch_bounds__(kBlock) batch_setup(BatchView B) {
+  const int r = replica_of(B, blockIdx.x);
+  const Replica& R = B.rep[r];
+  const int id = (blockIdx.x - R.cta_begin) * kBlock + threadIdx.x;
+  if (id >= R.g.vh) return;
+  curandStateMRG32k3a_t st;
+  curand_init(R.seed, (unsigned long long)(R.stream_off + id), 0ull, &st);
+  for (int p = 0; p < 2; p++) {
+    const Nbr n = make_nbr(R.g, id, p);
+    const bool frozen = R.bc == BC_PCC && at_y0(R.g, n);
+    for (int d = 0; d < 3; d++) {
+      Quat<double> u = q_one<double>();
+      if (R.hot && !(d != DIR_Y && frozen)) {
+        u.w = curand_uniform_double(&st) - 0.5;
+        u.x = curand_uniform_double(&st) - 0.5;
+        u.y = curand_uniform_double(&st) - 0.5;
+        u.z = curand_uniform_double(&st) - 0.5;
+        u = q_normalize(u);
+      }
+      if (FP64) {
+        Links64 L{B.lo + R.link_off, B.hi + R.link_off, R.g.vh};
+        L.st(d, p, id, u);
+      } else {
+        Links32 L{B.q32 + R.link_off, R.g.vh};
+        L.st(d, p, id, Quat<float>{(float)u.w, (float)u.x, (float)u.y, (float)u.z});
+      }
+    }
+  }
+  RngStore RS{B.rng + R.rng_off, R.g.vh};
+  RS.store(id, &st);
+}
+
+template <bool FP64>
+__global__ void __launch_bounds__(kBlock) batch_normalize(BatchView B) {
+  const int r = replica_of(B, blockIdx.x);
+  const Replica& R = B.rep[r];
+  const int id = (blockIdx.x - R.cta_begin) * kBlock + threadIdx.x;
+  if (id >= R.g.vh) return;
+  for (int p = 0; p < 2; p++)
+    for (int d = 0; d < 3; d++) {
+      if (FP64) {
+        Links64 L{B.lo + R.link_off, B.hi + R.link_off, R.g.vh};
+        L.st(d, p, id, q_normalize(L.ld_own(d, p, id)));
+      } else {
+        Links32 L{B.q32 + R.link_off, R.g.vh};
+        L.st(d, p, id, renorm_fast(L.ld_own(d, p, id)));
+      }
+    }
+}
+
+// energy / plaquette of every replica (en_av semantics, observables.h:99-141)
+// into series[r * cap + *cursor]; per-replica fixed-order sums as in measure<>
+template <bool FP64>
+__global__ void __launch_bounds__(kBlock) batch_measure(BatchView B, double2* partials, unsigned int* rep_count,
+                                                        unsigned int* all_count, int* cursor, double2* series,
+                                                        int cap) {
+  const int r = replica_of(B, blockIdx.x);
+  const Replica& R = B.rep[r];
+  const int id = (blockIdx.x - R.cta_begin) * kBlock + threadIdx.x;
+  const int k = *(volatile int*)cursor;  // advanced only by the last CTA below
+  double e = 0, pl = 0;
+  if (id < R.g.vh) {
+    for (int p = 0; p < 2; p++) {
+      const Nbr n = make_nbr(R.g, id, p);
+      double a, b, c;
+      if (FP64) {
+        Links64 L{B.lo + R.link_off, B.hi + R.link_off, R.g.vh};
+        a = plaq(L, DIR_Y, DIR_X, p, id, n.yp, n.xp);
+        b = plaq(L, DIR_Y, DIR_T, p, id, n.yp, n.tp);
+        c = plaq(L, DIR_X, DIR_T, p, id, n.xp, n.tp);
+      } else {
+        Links32 L{B.q32 + R.link_off, R.g.vh};
+        a = plaq(L, DIR_Y, DIR_X, p, id, n.yp, n.xp);
+        b = plaq(L, DIR_Y, DIR_T, p, id, n.yp, n.tp);
+        c = plaq(L, DIR_X, DIR_T, p, id, n.xp, n.tp);
+      }
+      if (R.bc == BC_PMC && at_ytop(R.g, n)) {
+        a = 0;
+        b = 0;
+      }
+      e += -c;
+      pl += (3 - a - b - c) / 3;
+    }
+  }
+  double se, sp;
+  block_sum2(e, pl, &se, &sp);
+  __shared__ bool last_rep, last_all;
+  const int nblk = (R.g.vh + kBlock - 1) / kBlock;
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = make_double2(se, sp);
+    __threadfence();
+    last_rep = atomicAdd(rep_count + r, 1u) == (unsigned int)nblk - 1;
+  }
+  __syncthreads();
+  if (last_rep) {
+    __threadfence();
+    double a = 0, b = 0;
+    for (int i = threadIdx.x; i < nblk; i += kBlock) {
+      double2 v = __ldcg(partials + R.cta_begin + i);
+      a += v.x;
+      b += v.y;
+    }
+    __syncthreads();
+    double sa, sb;
+    block_sum2(a, b, &sa, &sb);
+    if (threadIdx.x == 0) {
+      const double scale = 1.0 / (2.0 * (double)R.g.vh);
+      if (k < cap) series[(size_t)r * cap + k] = make_double2(sa * scale, sb * scale);
+      rep_count[r] = 0u;
+    }
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last_all = atomicAdd(all_count, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last_all && threadIdx.x == 0) {
+    *all_count = 0u;
+    *cursor = k + 1;
+  }
+}
+
+typedef void (*BatchPhaseFn)(BatchView, BatchArgs);
+
+template <int MU, int PAR, bool FP64>
+BatchPhaseFn pick_kind(int kind) {
+  return kind == KIND_HB ? batch_phase<MU, PAR, KIND_HB, FP64>
+         : kind == KIND_METRO ? batch_phase<MU, PAR, KIND_METRO, FP64>
+                              : batch_phase<MU, PAR, KIND_OR, FP64>;
+}
+
+template <bool FP64>
+BatchPhaseFn batch_phase_fn(int k, int kind) {
+  switch (k) {
+    case 0: return pick_kind<DIR_Y, 0, FP64>(kind);
+    case 1: return pick_kind<DIR_Y, 1, FP64>(kind);
+    case 2: return pick_kind<DIR_X, 0, FP64>(kind);
+    case 3: return pick_kind<DIR_X, 1, FP64>(kind);
+    case 4: return pick_kind<DIR_T, 0, FP64>(kind);
+    default: return pick_kind<DIR_T, 1, FP64>(kind);
+  }
+}
+
+}  // namespace
+
+struct qcd_batch {
+  std::vector<Replica> rep;
+  qcd_params common;
+  int n = 0;
+  long long sites = 0;
+  int ctas = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  Replica* rep_dev = nullptr;
+  float4* q32 = nullptr;
+  double2* lo = nullptr;
+  double2* hi = nullptr;
+  uint32_t* rng = nullptr;
+  int* accept = nullptr;
+  int* err = nullptr;
+  double2* partials = nullptr;
+  unsigned int* rep_count = nullptr;
+  unsigned int* all_count = nullptr;
+  int* cursor = nullptr;
+  double2* series = nullptr;
+  int cap = 0;
+  long long sweeps_done = 0;
+  cudaGraphExec_t graph = nullptr;
+  int graph_every = 0;
+  int graph_renorm_phase = -1;
+  char msg[512] = {0};
+};
+
+namespace {
+
+int bfail(qcd_batch* b, int code, const char* fmt, ...) {
+  if (b) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(b->msg, sizeof(b->msg), fmt, ap);
+    va_end(ap);
+  }
+  return code;
+}
+
+#define BCUDA(b, call)                                                                              \
+  do {                                                                                              \
+    cudaError_t e_ = (call);                                                                        \
+    if (e_ != cudaSuccess) {                                                                        \
+      cudaGetLastError();                                                                           \
+      return bfail(b, e_ == cudaErrorMemoryAllocation ? QCD_ERR_NOMEM : QCD_ERR_CUDA, "%s: %s", #call, \
+                   cudaGetErrorString(e_));                                                         \
+    }                                                                                               \
+  } while (0)
+
+BatchView view(const qcd_batch* b) { return BatchView{b->rep_dev, b->n, b->q32, b->lo, b->hi, b->rng}; }
+
+bool fp64(const qcd_batch* b) { return b->common.precision == QCD_PREC_FP64; }
+
+int batch_pass(qcd_batch* b, int kind, int renorm) {
+  BatchArgs a{b->common.epsilon, b->common.upd, b->err, b->accept, renorm};
+  for (int k = 0; k < 6; k++) {
+    if (fp64(b))
+      batch_phase_fn<true>(k, kind)<<<b->ctas, kBlock, 0, b->stream>>>(view(b), a);
+    else
+      batch_phase_fn<false>(k, kind)<<<b->ctas, kBlock, 0, b->stream>>>(view(b), a);
+    BCUDA(b, cudaGetLastError());
+  }
+  return QCD_OK;
+}
+
+// one sweep of every replica (+ n_or over-relaxation passes; FP32 links are
+// re-projected at their last update when `renorm`, FP64 by a normalize launch)
+int batch_sweep(qcd_batch* b, bool renorm) {
+  const int kind = b->common.algo == QCD_ALGO_HEATBATH ? KIND_HB : KIND_METRO;
+  const bool fused = renorm && !fp64(b);
+  int rc = batch_pass(b, kind, fused && b->common.n_or == 0);
+  for (int r = 0; rc == QCD_OK && r < b->common.n_or; r++) rc = batch_pass(b, KIND_OR, fused && r == b->common.n_or - 1);
+  if (rc) return rc;
+  if (renorm && !fused) {
+    if (fp64(b))
+      batch_normalize<true><<<b->ctas, kBlock, 0, b->stream>>>(view(b));
+    else
+      batch_normalize<false><<<b->ctas, kBlock, 0, b->stream>>>(view(b));
+    BCUDA(b, cudaGetLastError());
+  }
+  return QCD_OK;
+}
+
+int batch_measure_launch(qcd_batch* b) {
+  if (fp64(b))
+    batch_measure<true><<<b->ctas, kBlock, 0, b->stream>>>(view(b), b->partials, b->rep_count, b->all_count,
+                                                            b->cursor, b->series, b->cap);
+  else
+    batch_measure<false><<<b->ctas, kBlock, 0, b->stream>>>(view(b), b->partials, b->rep_count, b->all_count,
+                                                             b->cursor, b->series, b->cap);
+  BCUDA(b, cudaGetLastError());
+  return QCD_OK;
+}
+
+bool renorm_due(const qcd_batch* b, long long sweep_index) {
+  return b->common.renorm_every > 0 && (sweep_index + 1) % b->common.renorm_every == 0;
+}
+
+void release(qcd_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  cudaFree(b->rep_dev);
+  cudaFree(b->q32);
+  cudaFree(b->lo);
+  cudaFree(b->hi);
+  cudaFree(b->rng);
+  cudaFree(b->accept);
+  cudaFree(b->err);
+  cudaFree(b->partials);
+  cudaFree(b->rep_count);
+  cudaFree(b->all_count);
+  cudaFree(b->cursor);
+  cudaFree(b->series);
+  if (b->own) cudaStreamDestroy(b->own);
+}
+
+}  // namespace
+
+extern "C" {
+
+int qcd_batch_create(const qcd_replica* r, int n, const qcd_params* common, qcd_batch** out) {
+  if (!r || n < 1 || !common || !out) return QCD_ERR_INVALID;
+  *out = nullptr;
+  if (common->algo != QCD_ALGO_HEATBATH && common->algo != QCD_ALGO_METROPOLIS) return QCD_ERR_INVALID;
+  if (common->precision != QCD_PREC_FP64 && common->precision != QCD_PREC_FP32) return QCD_ERR_INVALID;
+  if (common->n_or < 0 || common->renorm_every < 0 || common->upd < 0) return QCD_ERR_INVALID;
+  if (common->algo == QCD_ALGO_METROPOLIS && !(common->epsilon > 0.f && common->epsilon < 1.f)) return QCD_ERR_INVALID;
+  qcd_batch* b = new (std::nothrow) qcd_batch();
+  if (!b) return QCD_ERR_NOMEM;
+  b->common = *common;
+  b->n = n;
+  long long link_off = 0, rng_off = 0, site_off = 0;
+  int cta = 0;
+  for (int i = 0; i < n; i++) {
+    const qcd_replica& x = r[i];
+    if (x.lt < 2 || x.lx < 2 || x.ly < 2 || (x.lt & 1) || (x.lx & 1) || (x.ly & 1) || !(x.beta > 0.f) ||
+        x.boundary < 0 || x.boundary > 2 || x.stream_offset < 0) {
+      delete b;
+      return QCD_ERR_INVALID;
+    }
+    const long long V = (long long)x.lt * x.lx * x.ly;
+    if (V / 2 >= (1ll << 31) / 6) {
+      delete b;
+      return QCD_ERR_INVALID;
+    }
+    Replica R;
+    R.g = make_geo(x.lt, x.lx, x.ly);
+    R.beta = x.beta;
+    R.bc = x.boundary;
+    R.hot = x.hot;
+    R.link_off = link_off;
+    R.rng_off = rng_off;
+    R.site_off = site_off;
+    R.cta_begin = cta;
+    R.seed = x.seed;
+    R.stream_off = x.stream_offset;
+    b->rep.push_back(R);
+    link_off += 6 * (V / 2);
+    rng_off += 6 * (V / 2);
+    site_off += V;
+    cta += (int)((V / 2 + kBlock - 1) / kBlock);
+  }
+  b->sites = site_off;
+  b->ctas = cta;
+  int rc = QCD_OK;
+  auto step = [&](cudaError_t e, const char* what) {
+    if (rc == QCD_OK && e != cudaSuccess) {
+      rc = e == cudaErrorMemoryAllocation ? QCD_ERR_NOMEM : QCD_ERR_CUDA;
+      cudaGetLastError();
+      snprintf(b->msg, sizeof(b->msg), "%s: %s", what, cudaGetErrorString(e));
+    }
+  };
+  step(cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking), "cudaStreamCreate");
+  b->stream = b->own;
+  if (rc == QCD_OK) step(cudaMalloc(&b->rep_dev, n * sizeof(Replica)), "cudaMalloc(replicas)");
+  if (rc == QCD_OK)
+    step(cudaMemcpy(b->rep_dev, b->rep.data(), n * sizeof(Replica), cudaMemcpyHostToDevice), "replica table");
+  if (common->precision == QCD_PREC_FP64) {
+    if (rc == QCD_OK) step(cudaMalloc(&b->lo, link_off * sizeof(double2)), "cudaMalloc(links)");
+    if (rc == QCD_OK) step(cudaMalloc(&b->hi, link_off * sizeof(double2)), "cudaMalloc(links)");
+  } else if (rc == QCD_OK) {
+    step(cudaMalloc(&b->q32, link_off * sizeof(float4)), "cudaMalloc(links)");
+  }
+  if (rc == QCD_OK) step(cudaMalloc(&b->rng, rng_off * sizeof(uint32_t)), "cudaMalloc(rng)");
+  if (rc == QCD_OK && common->algo == QCD_ALGO_METROPOLIS) {
+    step(cudaMalloc(&b->accept, site_off * sizeof(int)), "cudaMalloc(accept)");
+    if (rc == QCD_OK) step(cudaMemsetAsync(b->accept, 0, site_off * sizeof(int), b->stream), "memset");
+  }
+  if (rc == QCD_OK) step(cudaMalloc(&b->err, sizeof(int)), "cudaMalloc(err)");
+  if (rc == QCD_OK) step(cudaMalloc(&b->partials, (size_t)cta * sizeof(double2)), "cudaMalloc(partials)");
+  if (rc == QCD_OK) step(cudaMalloc(&b->rep_count, n * sizeof(unsigned int)), "cudaMalloc(counters)");
+  if (rc == QCD_OK) step(cudaMalloc(&b->all_count, sizeof(unsigned int)), "cudaMalloc(counters)");
+  if (rc == QCD_OK) step(cudaMalloc(&b->cursor, sizeof(int)), "cudaMalloc(cursor)");
+  if (rc == QCD_OK) step(cudaMemsetAsync(b->err, 0, sizeof(int), b->stream), "memset");
+  if (rc == QCD_OK) step(cudaMemsetAsync(b->rep_count, 0, n * sizeof(unsigned int), b->stream), "memset");
+  if (rc == QCD_OK) step(cudaMemsetAsync(b->all_count, 0, sizeof(unsigned int), b->stream), "memset");
+  if (rc == QCD_OK) step(cudaMemsetAsync(b->cursor, 0, sizeof(int), b->stream), "memset");
+  if (rc == QCD_OK) step(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize");
+  if (rc != QCD_OK) {
+    fprintf(stderr, "qcd_batch_create: %s\n", b->msg);
+    release(b);
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return QCD_OK;
+}
+
+int qcd_batch_destroy(qcd_batch* b) {
+  if (!b) return QCD_ERR_INVALID;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  release(b);
+  delete b;
+  return QCD_OK;
+}
+
+int qcd_batch_set_stream(qcd_batch* b, void* stream) {
+  if (!b) return QCD_ERR_INVALID;
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  b->stream = stream ? (cudaStream_t)stream : b->own;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  return QCD_OK;
+}
+
+int qcd_batch_init(qcd_batch* b) {
+  if (!b) return QCD_ERR_INVALID;
+  if (fp64(b))
+    batch_setup<true><<<b->ctas, kBlock, 0, b->stream>>>(view(b));
+  else
+    batch_setup<false><<<b->ctas, kBlock, 0, b->stream>>>(view(b));
+  BCUDA(b, cudaGetLastError());
+  BCUDA(b, cudaMemsetAsync(b->cursor, 0, sizeof(int), b->stream));
+  b->sweeps_done = 0;
+  return QCD_OK;
+}
+
+int qcd_batch_reserve(qcd_batch* b, int capacity) {
+  if (!b || capacity < 0) return QCD_ERR_INVALID;
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  cudaFree(b->series);
+  b->series = nullptr;
+  b->cap = 0;
+  if (b->graph) {  // the graph holds the old series pointer
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  if (capacity) {
+    BCUDA(b, cudaMalloc(&b->series, (size_t)capacity * b->n * sizeof(double2)));
+    BCUDA(b, cudaMemsetAsync(b->series, 0, (size_t)capacity * b->n * sizeof(double2), b->stream));
+  }
+  BCUDA(b, cudaMemsetAsync(b->cursor, 0, sizeof(int), b->stream));
+  b->cap = capacity;
+  return QCD_OK;
+}
+
+int qcd_batch_run(qcd_batch* b, int sweeps, int measure_every, int use_graph) {
+  if (!b || sweeps < 0 || measure_every < 0) return QCD_ERR_INVALID;
+  if (measure_every > 0 && b->cap == 0) return bfail(b, QCD_ERR_INVALID, "reserve a series before measuring");
+  int rc = QCD_OK;
+  // a graph of one measurement interval; its re-projection pattern must not
+  // vary between replays, so it is used when renorm_every divides the interval
+  const int every = measure_every > 0 ? measure_every : 1;
+  const bool graphable = use_graph && measure_every > 0 &&
+                         (b->common.renorm_every == 0 || every % b->common.renorm_every == 0) &&
+                         b->sweeps_done % every == 0 &&
+                         (b->common.renorm_every == 0 || b->sweeps_done % b->common.renorm_every == 0);
+  int done = 0;
+  if (graphable && sweeps >= every) {
+    if (!b->graph || b->graph_every != every) {
+      if (b->graph) cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+      cudaGraph_t g;
+      BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      for (int s = 0; rc == QCD_OK && s < every; s++) rc = batch_sweep(b, renorm_due(b, s));
+      if (rc == QCD_OK) rc = batch_measure_launch(b);
+      cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+      if (rc) {
+        if (e == cudaSuccess) cudaGraphDestroy(g);
+        return rc;
+      }
+      BCUDA(b, e);
+      e = cudaGraphInstantiate(&b->graph, g, 0);
+      cudaGraphDestroy(g);
+      BCUDA(b, e);
+      b->graph_every = every;
+    }
+    for (; done + every <= sweeps; done += every) {
+      BCUDA(b, cudaGraphLaunch(b->graph, b->stream));
+      b->sweeps_done += every;
+    }
+  }
+  for (; done < sweeps; done++) {
+    rc = batch_sweep(b, renorm_due(b, b->sweeps_done));
+    if (rc) return rc;
+    b->sweeps_done++;
+    if (measure_every > 0 && b->sweeps_done % measure_every == 0) {
+      rc = batch_measure_launch(b);
+      if (rc) return rc;
+    }
+  }
+  return QCD_OK;
+}
+
+int qcd_batch_synchronize(qcd_batch* b) {
+  if (!b) return QCD_ERR_INVALID;
+  int e = 0;
+  BCUDA(b, cudaMemcpyAsync(&e, b->err, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  if (e & DEVERR_HB_LOOP)
+    return bfail(b, QCD_ERR_NONUNITARY, "heat-bath rejection loop exceeded %d tries", QCD_HB_MAX_TRIES);
+  return QCD_OK;
+}
+
+int qcd_batch_measured(qcd_batch* b) {
+  if (!b) return QCD_ERR_INVALID;
+  int k = 0;
+  BCUDA(b, cudaMemcpyAsync(&k, b->cursor, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  return k;
+}
+
+int qcd_batch_series(qcd_batch* b, int replica, double* energy, double* plaquette, int n) {
+  if (!b || replica < 0 || replica >= b->n || n < 0 || n > b->cap) return QCD_ERR_INVALID;
+  int rc = qcd_batch_synchronize(b);
+  if (rc) return rc;
+  if (n == 0) return QCD_OK;
+  std::vector<double2> tmp(n);
+  BCUDA(b, cudaMemcpy(tmp.data(), b->series + (size_t)replica * b->cap, n * sizeof(double2), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < n; i++) {
+    if (energy) energy[i] = tmp[i].x;
+    if (plaquette) plaquette[i] = tmp[i].y;
+  }
+  return QCD_OK;
+}
+
+int qcd_batch_store_config(qcd_batch* b, int replica, double* aos_host) {
+  if (!b || !aos_host || replica < 0 || replica >= b->n) return QCD_ERR_INVALID;
+  int rc = qcd_batch_synchronize(b);
+  if (rc) return rc;
+  const Replica& R = b->rep[replica];
+  const size_t vh = (size_t)R.g.vh;
+  // SoA planes -> the reference's AoS layout, on the host
+  if (fp64(b)) {
+    std::vector<double2> lo(6 * vh), hi(6 * vh);
+    BCUDA(b, cudaMemcpy(lo.data(), b->lo + R.link_off, 6 * vh * sizeof(double2), cudaMemcpyDeviceToHost));
+    BCUDA(b, cudaMemcpy(hi.data(), b->hi + R.link_off, 6 * vh * sizeof(double2), cudaMemcpyDeviceToHost));
+    for (int p = 0; p < 2; p++)
+      for (size_t id = 0; id < vh; id++)
+        for (int d = 0; d < 3; d++) {
+          const size_t i = (size_t)(d * 2 + p) * vh + id;
+          double* s = aos_host + ((size_t)p * vh + id) * 12 + d * 4;
+          s[0] = lo[i].x;
+          s[1] = lo[i].y;
+          s[2] = hi[i].x;
+          s[3] = hi[i].y;
+        }
+  } else {
+    std::vector<float4> q(6 * vh);
+    BCUDA(b, cudaMemcpy(q.data(), b->q32 + R.link_off, 6 * vh * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (int p = 0; p < 2; p++)
+      for (size_t id = 0; id < vh; id++)
+        for (int d = 0; d < 3; d++) {
+          const float4 u = q[(size_t)(d * 2 + p) * vh + id];
+          double* s = aos_host + ((size_t)p * vh + id) * 12 + d * 4;
+          s[0] = u.x;
+          s[1] = u.y;
+          s[2] = u.z;
+          s[3] = u.w;
+        }
+  }
+  return QCD_OK;
+}
+
+long long qcd_batch_sites(const qcd_batch* b) { return b ? b->sites : 0; }
+
+const char* qcd_batch_last_error(const qcd_batch* b) { return b ? b->msg : "null batch"; }
+
+}  // extern "C"

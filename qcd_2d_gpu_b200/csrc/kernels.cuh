@@ -8,83 +8,9 @@
 #include "rng.cuh"
 #include "su2.cuh"
 #include "updates.cuh"
+#include "sites.cuh"
 
 namespace qcd {
-
-constexpr int kBlock = 256;
-
-struct PhaseArgs {
-  float beta;
-  float eps;
-  int upd;
-  int* err;     // device error word
-  int* accept;  // V ints, reference site order; only for Metropolis
-  int renorm;   // FP32: re-project each updated link (in double) before it is stored
-};
-
-// ------------------------------------------------------- one link update --
-// Update U_MU at site n of sublattice PAR: the body of the six launches of
-// mc_up_per/pcc/pmc (mc_updates.h:129-465, mc_updates_pcc.h:4-214,
-// mc_updates_pmc.h:4-247).  Shared by the per-phase kernels (CG = false) and
-// the wavefront kernel (CG = true).
-template <bool CG>
-__device__ __forceinline__ void add_accept(int* p, int v) {
-  if (CG)
-    atomicAdd(p, v);  // at L2: the counter may sit in a stale L1 line
-  else
-    *p += v;
-}
-
-template <int MU, int PAR, int BC, int KIND, bool CG>
-__device__ __forceinline__ void site64(const Links64T<CG>& L, const RngStoreT<CG>& R, const Geo& g,
-                                       const PhaseArgs& a, const Nbr& n) {
-  if (BC == BC_PCC && MU != DIR_Y && at_y0(g, n)) return;
-  const int id = n.id;
-  Quat<double> A = staple_sum<MU, BC, Links64T<CG>, double>(L, g, n, PAR);
-  if (KIND == KIND_HB) {
-    curandStateMRG32k3a_t st;
-    R.load(id, &st);
-    Quat<double> U = heatbath_ref(A, (double)a.beta, &st, a.err);
-    L.st(MU, PAR, id, U);
-    R.store(id, &st);
-  } else if (KIND == KIND_METRO) {
-    curandStateMRG32k3a_t st;
-    R.load(id, &st);
-    Quat<double> U = L.ld_own(MU, PAR, id);
-    int acc = metropolis_ref(U, A, (double)a.beta, (double)a.eps, a.upd, &st);
-    L.st(MU, PAR, id, U);
-    R.store(id, &st);
-    add_accept<CG>(a.accept + PAR * g.vh + id, acc);
-  } else {
-    Quat<double> U = L.ld_own(MU, PAR, id);
-    L.st(MU, PAR, id, overrelax_ref(A, U));
-  }
-}
-
-template <int MU, int PAR, int BC, int KIND, bool CG>
-__device__ __forceinline__ void site32(const Links32T<CG>& L, const RngStoreT<CG>& R, const Geo& g,
-                                       const PhaseArgs& a, const Nbr& n, int renorm) {
-  if (BC == BC_PCC && MU != DIR_Y && at_y0(g, n)) return;
-  const int id = n.id;
-  Quat<float> A = staple_sum<MU, BC, Links32T<CG>, float>(L, g, n, PAR);
-  Quat<float> U;
-  if (KIND == KIND_HB) {
-    curandStateMRG32k3a_t st;
-    R.load(id, &st);
-    U = heatbath_fast(A, a.beta, &st, a.err);
-    R.store(id, &st);
-  } else if (KIND == KIND_METRO) {
-    curandStateMRG32k3a_t st;
-    R.load(id, &st);
-    U = L.ld_own(MU, PAR, id);
-    int acc = metropolis_fast(U, A, a.beta, a.eps, a.upd, &st);
-    R.store(id, &st);
-    add_accept<CG>(a.accept + PAR * g.vh + id, acc);
-  } else {
-    U = overrelax_fast(A, L.ld_own(MU, PAR, id));
-  }
-  L.st(MU, PAR, id, renorm ? renorm_fast(U) : U);
-}
 
 // ------------------------------------------------------------ one phase --
 // Launch grid (ceil(slice / kBlock), Lt): blockIdx.y is the t-slice.
@@ -225,93 +151,6 @@ __global__ void __launch_bounds__(kBlock) soa_to_aos32(Links32 L, double* __rest
       s[d * 4 + 3] = u.z;
     }
   }
-}
-
-// ---------------------------------------------------------- reductions --
-// Deterministic FP64 sums: each CTA writes its partial (fixed tree order),
-// the last CTA to finish adds the partials in index order and resets the
-// arrival counter.  No floating-point atomics, so the result does not depend
-// on CTA scheduling (the reference's en_av uses atomicAdd, observables.h:137-140).
-__device__ __forceinline__ double warp_sum(double v) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// Sums two values over the CTA into out2 (valid in thread 0).
-__device__ __forceinline__ void block_sum2(double v0, double v1, double* out0, double* out1) {
-  __shared__ double sh[2][kBlock / 32];
-  v0 = warp_sum(v0);
-  v1 = warp_sum(v1);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) {
-    sh[0][w] = v0;
-    sh[1][w] = v1;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0, b = 0;
-    for (int i = 0; i < kBlock / 32; i++) {
-      a += sh[0][i];
-      b += sh[1][i];
-    }
-    *out0 = a;
-    *out1 = b;
-  }
-}
-
-// After thread 0 of every CTA stored its partial pair: the last CTA adds all
-// partials in order, scales them and writes out[0..1].
-__device__ __forceinline__ void finish_sum2(double2* partials, unsigned int* counter, double scale,
-                                            double* out) {
-  __shared__ bool last;
-  if (threadIdx.x == 0) {
-    __threadfence();
-    unsigned int prev = atomicAdd(counter, 1u);
-    last = (prev == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  // fixed-order sum over partials: per-thread strided chunks, then the CTA tree
-  double a = 0, b = 0;
-  for (unsigned int i = threadIdx.x; i < gridDim.x; i += kBlock) {
-    double2 v = __ldcg(partials + i);  // L2: written by other CTAs
-    a += v.x;
-    b += v.y;
-  }
-  __syncthreads();
-  double sa, sb;
-  block_sum2(a, b, &sa, &sb);
-  if (threadIdx.x == 0) {
-    out[0] = sa * scale;
-    out[1] = sb * scale;
-    *counter = 0u;
-  }
-}
-
-// 1 - 1/2 Re tr of the plaquettes at one site, in the reference's product
-// order (plaquette_yx/yt/xt, observables.h:1-21):
-//   P_yx = U_y(x) U_x(x+y) U_y(x+x)^+ U_x(x)^+  and alike.
-template <class L>
-__device__ __forceinline__ Quat<double> ld64(const L& links, int d, int p, int id);
-template <>
-__device__ __forceinline__ Quat<double> ld64<Links64>(const Links64& links, int d, int p, int id) {
-  return links.ld(d, p, id);
-}
-template <>
-__device__ __forceinline__ Quat<double> ld64<Links32>(const Links32& links, int d, int p, int id) {
-  Quat<float> u = links.ld(d, p, id);
-  return Quat<double>{u.w, u.x, u.y, u.z};
-}
-
-template <class L>
-__device__ __forceinline__ double plaq(const L& links, int mu, int nu, int p, int id, int omu,
-                                       int onu) {
-  // U_mu(x) U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+
-  Quat<double> A = q_mul(ld64(links, mu, p, id), ld64(links, nu, p ^ 1, id + omu));
-  Quat<double> B = q_mul_bd(A, ld64(links, mu, p ^ 1, id + onu));
-  A = q_mul_bd(B, ld64(links, nu, p, id));
-  return 1 - A.w;
 }
 
 // en_av<PMC> (observables.h:99-141): energy = mean of -(1 - P_xt), plaquette
