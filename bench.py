@@ -93,6 +93,151 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+C4_SWEEPS = 200
+
+
+def c4_replicas():
+    """96 replicas: Nt = Nx uniform over even 8..64, Ny over even 8..128, beta
+    uniform in [3, 12], boundary r mod 3, hot start for even r, seed 1234 + r
+    (numpy's PCG64 seeded with 1234 draws the shapes)."""
+    import numpy as np
+
+    rng = np.random.default_rng(1234)
+    reps = []
+    for r in range(96):
+        lt = int(rng.choice(np.arange(8, 65, 2)))
+        ly = int(rng.choice(np.arange(8, 129, 2)))
+        beta = float(rng.uniform(3.0, 12.0))
+        reps.append(dict(lt=lt, lx=lt, ly=ly, beta=beta, boundary=r % 3, hot=int(r % 2 == 0), seed=1234 + r,
+                         stream_offset=0))
+    return reps
+
+
+def run_batch_c4(q, torch, stream):
+    """Batched replicas: the 96 lattices in shared launches, FP32 heat-bath,
+    a measurement every sweep, the interval replayed as a CUDA graph; timed
+    from the seeding of the streams to the last measurement."""
+    reps = c4_replicas()
+    sites = sum(r["lt"] * r["lx"] * r["ly"] for r in reps)
+    B = q.Batch(reps, algo="hb", precision="fp32", renorm_every=1)
+    B.set_stream(stream.cuda_stream)
+    B.reserve(C4_SWEEPS)
+    B.init()
+    B.run(3, measure_every=1)  # warm-up: graph capture and first launches
+    B.synchronize()
+    B.reserve(C4_SWEEPS)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    B.init()
+    B.run(C4_SWEEPS, measure_every=1, graph=True)
+    e1.record(stream)
+    B.synchronize()
+    ms = e0.elapsed_time(e1)
+    assert B.measured() == C4_SWEEPS
+    B.close()
+    return {"workload": f"96 replicas (Nt=Nx in 8..64, Ny in 8..128, beta in [3,12], bc r mod 3, half hot), "
+                        f"FP32 heat-bath, {C4_SWEEPS} sweeps with a measurement each, CUDA graph",
+            "replicas_per_s": len(reps) / (ms * 1e-3), "link_updates_per_s": 3.0 * sites * C4_SWEEPS / (ms * 1e-3),
+            "ms": ms, "sites": sites}
+
+
+def reference_accuracy(args):
+    """The reference's own build on the accuracy-scan runs: its link updates/s
+    per (boundary, beta) at the scan size (heat-bath sweeps with en_av each)."""
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built"}))
+        return 0
+    L3 = args.scan_size
+    for bc in (0, 2):
+        for beta in (4.0, 6.0, 8.0, 10.0, 12.0):
+            out = subprocess.run([harness, "bench", "--lt", str(L3), "--lx", str(L3), "--ly", str(L3), "--algo", "hb",
+                                  "--bc", str(bc), "--hot", "0", "--beta", str(beta), "--sweeps", "200", "--warmup",
+                                  "20"], capture_output=True, text=True, check=True)
+            r = json.loads(out.stdout.strip().splitlines()[-1])
+            ms = r["ms_per_sweep"] + r["ms_measure"]
+            print(json.dumps({"impl": "reference", "lattice": [L3] * 3, "boundary": bc, "beta": beta,
+                              "link_updates_per_s": 3.0 * L3 ** 3 / (ms * 1e-3), "ms_per_sweep_with_measure": ms}))
+    return 0
+
+
+def reference_batch_c4(harness):
+    import tempfile
+
+    reps = c4_replicas()
+    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
+        for r in reps:
+            f.write(f"{r['lt']} {r['lx']} {r['ly']} {r['beta']!r} {r['boundary']} {r['hot']} {r['seed']}\n")
+        name = f.name
+    try:
+        out = subprocess.run([harness, "batch", "--list", name, "--sweeps", str(C4_SWEEPS)], capture_output=True,
+                             text=True, check=True)
+    finally:
+        os.unlink(name)
+    r = json.loads(out.stdout.strip().splitlines()[-1])
+    return {"workload": f"the same 96 replicas run one after the other by the reference's kernels (FP64 "
+                        f"heat-bath, {C4_SWEEPS} sweeps, en_av each sweep)",
+            "replicas_per_s": r["replicas_per_s"], "link_updates_per_s": r["link_updates_per_s"], "ms": r["ms_total"],
+            "sites": r["sites"]}
+
+
+def accuracy_scan(args, q, torch):
+    """FP32 + FP64 fix-ups against FP64 at 128^3, periodic and PMC, beta in
+    {4, 6, 8, 10, 12}: `--scan-sweeps` heat-bath sweeps from a cold start
+    (the first fifth discarded), a measurement every sweep; binned means and
+    errors, tau_int (Madras-Sokal, c = 6) and link updates/s per variant.
+    The FP64 path reproduces the reference's build bit for bit (the golden
+    tests), so its series stand for the reference's long runs; with
+    --impl reference the reference's own build is timed on the same runs."""
+    import numpy as np
+
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    L3 = args.scan_size
+    sweeps = args.scan_sweeps
+    therm = sweeps // 5
+    out = []
+    for bc in (0, 2):
+        for beta in (4.0, 6.0, 8.0, 10.0, 12.0):
+            row = {"lattice": [L3] * 3, "boundary": bc, "beta": beta, "sweeps": sweeps, "discarded": therm}
+            for prec in ("fp64", "fp32"):
+                lat = q.Lattice(L3, L3, L3, beta, boundary=bc, precision=prec,
+                                renorm_every=1 if prec == "fp32" else 0, seed=2026)
+                lat.set_stream(stream.cuda_stream)
+                lat.init_cold()
+                lat.series_reserve(sweeps)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for i in range(sweeps):
+                    if prec == "fp64" and (i + 1) % 100 == 0:
+                        lat.normalize()  # the reference re-projects every 100 sweeps
+                    lat.sweep(1)
+                    lat.measure_into_series(i)
+                e1.record(stream)
+                e, p = lat.series_read(sweeps)
+                ms = e0.elapsed_time(e1)
+                lat.close()
+                res = {"link_updates_per_s": 3.0 * L3 ** 3 * sweeps / (ms * 1e-3)}
+                for name, x in (("plaquette", p[therm:]), ("energy", e[therm:])):
+                    tau, w, dtau = q.tau_int(x, 6.0)
+                    b = max(1, int(np.ceil(4 * tau)))
+                    m, err = q.binned(x, b)
+                    res[name] = {"mean": m, "err": err, "tau_int": tau, "dtau": dtau, "bin": b}
+                row[prec] = res
+            for name in ("plaquette", "energy"):
+                a, b = row["fp64"][name], row["fp32"][name]
+                d = abs(a["mean"] - b["mean"])
+                row[f"delta_{name}"] = d
+                row[f"delta_{name}_sigma"] = d / float(np.hypot(a["err"], b["err"]))
+            out.append(row)
+            print(json.dumps(row), flush=True)
+    n2 = sum(1 for r in out for k in ("plaquette", "energy") if r[f"delta_{k}_sigma"] <= 2.0)
+    print(json.dumps({"summary": f"{n2} of {2 * len(out)} FP32-vs-FP64 comparisons within 2 sigma",
+                      "max_delta_plaquette": max(r["delta_plaquette"] for r in out),
+                      "max_delta_energy": max(r["delta_energy"] for r in out)}))
+    return 0
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -155,6 +300,7 @@ def reference_arm(args, ws, rank):
                                    "with CUDA events (the reference has no CPU implementation)"},
         "e2e": {"value": ups, "unit": "link updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_raw": r,
+        "batched": reference_batch_c4(harness),
     })
     print(json.dumps(line))
     return 0
@@ -167,7 +313,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-replica measurement")
     ap.add_argument("--lattice", type=int, nargs=3, default=None, help="override (testing only)")
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "accuracy"])
+    ap.add_argument("--scan-size", type=int, default=128)
+    ap.add_argument("--scan-sweeps", type=int, default=2000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -176,6 +326,14 @@ def main():
         global LT, LX, LY
         LT, LX, LY = args.lattice
 
+    if args.workload == "accuracy":
+        if args.impl == "reference":
+            return reference_accuracy(args)
+        import torch
+
+        import qcd_2d_gpu_b200 as q
+
+        return accuracy_scan(args, q, torch)
     if args.impl == "reference":
         return reference_arm(args, ws, rank)
 
@@ -305,6 +463,8 @@ def main():
     e2e_value = updates_per_step * args.steps * ws / (e2e_ms * 1e-3)
     E.close()
 
+    batched = run_batch_c4(q, torch, stream) if not args.no_batch else None
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = run_cpu_baseline()
@@ -338,6 +498,7 @@ def main():
                     "note": "one AoS FP64 configuration uploaded from pinned host memory per timed run "
                             "(amortised over the steps); one (energy, plaquette) readback per step"},
             "gpu_launches": launches_per_step * args.steps,
+            "batched": batched,
             "clocks": clk.summary(),
         }
         print(json.dumps(line))

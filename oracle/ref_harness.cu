@@ -31,6 +31,7 @@
 #include <string.h>
 #include <math.h>
 #include <time.h>
+#include <algorithm>
 #include <vector>
 #include <string>
 #include <cuda_runtime.h>
@@ -139,6 +140,7 @@ struct Args {
   int readconf = 0, sconf = 0, save = 0, N = 100, N_term = 10, N_block = 20, Nblock_term = 10, Nsave = 5,
       N_cor = 1, W = 10;
   std::string nsave = "1", nconfr = "1", nconfs = "1";
+  std::string list;  // mode "batch": one replica per line "lt lx ly beta bc hot seed"
 };
 
 static void usage() {
@@ -202,6 +204,7 @@ static Args parse(int argc, char** argv) {
     else if (k == "--nsave") a.nsave = v;
     else if (k == "--nconfr") a.nconfr = v;
     else if (k == "--nconfs") a.nconfs = v;
+    else if (k == "--list") a.list = v;
     else usage();
   }
   return a;
@@ -541,6 +544,71 @@ DEFINE_MAIN(ref_hb)
 DEFINE_MAIN(ref_metro)
 
 
+
+// Mode "batch": the replicas of a list run one after the other, each exactly
+// as one run of the reference program would run it (setup_kernel, start,
+// `sweeps` x (mc_up_* + en_av)), timed on the device from the first replica's
+// setup to the last replica's last measurement (allocation excluded).
+static int batch_main(const Args& a) {
+  FILE* f = fopen(a.list.c_str(), "r");
+  if (!f) {
+    fprintf(stderr, "cannot read %s\n", a.list.c_str());
+    return 2;
+  }
+  struct Rep { int lt, lx, ly, bc, hot; double beta; long long seed; };
+  std::vector<Rep> reps;
+  Rep r;
+  while (fscanf(f, "%d %d %d %lf %d %d %lld", &r.lt, &r.lx, &r.ly, &r.beta, &r.bc, &r.hot, &r.seed) == 7)
+    reps.push_back(r);
+  fclose(f);
+  size_t max_v = 0;
+  for (const Rep& x : reps) max_v = std::max(max_v, (size_t)x.lt * x.lx * x.ly);
+  curandStateMRG32k3a_t* st;
+  double *phid, *end, *end2;
+  int* acc;
+  CK(cudaMalloc((void**)&st, max_v / 2 * sizeof(curandStateMRG32k3a_t)));
+  CK(cudaMalloc(&phid, max_v * 12 * sizeof(double)));
+  CK(cudaMalloc(&acc, max_v * sizeof(int)));
+  CK(cudaMalloc(&end, a.sweeps * sizeof(double)));
+  CK(cudaMalloc(&end2, a.sweeps * sizeof(double)));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  double sites = 0;
+  CK(cudaDeviceSynchronize());
+  CK(cudaEventRecord(e0));
+  for (const Rep& x : reps) {
+    ref_hb::lattice l2 = {x.ly / 2, x.lx, x.lt, x.lt * x.lx * x.ly / 2, 3, 4, 12, (float)x.beta, (float)a.eps, a.upd};
+    int nthreads = 256;  // kernel.cu:66-70
+    while (l2.V % nthreads != 0) nthreads--;
+    int nblocks = 2 * (l2.V / nthreads);
+    ref_hb::setup_kernel<<<nblocks / 2, nthreads>>>(st, (int)x.seed);
+    if (x.hot) {
+      if (x.bc == 1) ref_hb::rand_init2_pcc<<<nblocks / 2, nthreads>>>(phid, st, l2);
+      else ref_hb::rand_init2<<<nblocks / 2, nthreads>>>(phid, st, l2);
+    } else {
+      ref_hb::id_init2<<<nblocks / 2, nthreads>>>(phid, l2);
+    }
+    CK(cudaMemsetAsync(end, 0, a.sweeps * sizeof(double)));
+    CK(cudaMemsetAsync(end2, 0, a.sweeps * sizeof(double)));
+    for (int i = 0; i < a.sweeps; i++) {
+      ref_hb_sweep(x.bc, 0, nblocks, nthreads, phid, st, acc, l2);
+      if (x.bc == 2) ref_hb::en_av<1><<<nblocks, nthreads>>>(phid, end + i, end2 + i, l2);
+      else ref_hb::en_av<0><<<nblocks, nthreads>>>(phid, end + i, end2 + i, l2);
+    }
+    sites += 2.0 * l2.V;
+  }
+  CK(cudaEventRecord(e1));
+  CK(cudaEventSynchronize(e1));
+  CK(cudaGetLastError());
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  printf("{\"ms_total\": %.6f, \"replicas\": %zu, \"sweeps\": %d, \"sites\": %.0f, \"replicas_per_s\": %.6e, "
+         "\"link_updates_per_s\": %.6e}\n",
+         ms, reps.size(), a.sweeps, sites, reps.size() / (ms * 1e-3), 3.0 * sites * a.sweeps / (ms * 1e-3));
+  return 0;
+}
+
 int main(int argc, char** argv) {
   Args a = parse(argc, argv);
   if (a.mode == "tape") {
@@ -561,6 +629,7 @@ int main(int argc, char** argv) {
     cudaFree(d);
     return 0;
   }
+  if (a.mode == "batch") return batch_main(a);
   if (a.mode == "main") return a.algo == METROPOLIS ? ref_metro_kernel_main(a) : ref_hb_kernel_main(a);
   if (a.mode != "run" && a.mode != "bench") usage();
   // over-relaxation (update==1) and heat-bath share the HEATBATH namespace: the
