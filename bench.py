@@ -317,6 +317,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-replica measurement")
     ap.add_argument("--lattice", type=int, nargs=3, default=None, help="override (testing only)")
     ap.add_argument("--workload", default="sweep", choices=["sweep", "accuracy"])
+    ap.add_argument("--schedule", default="auto", choices=["auto", "phases", "wavefront"])
+    ap.add_argument("--wave-tuning", type=int, nargs=3, default=None, metavar=("CHUNK", "PASSES", "FRONTS"))
     ap.add_argument("--scan-size", type=int, default=128)
     ap.add_argument("--scan-sweeps", type=int, default=2000)
     args = ap.parse_args()
@@ -360,7 +362,12 @@ def main():
     L = q.Lattice(LT, LX, LY, BETA, algo="hb", boundary="pmc", precision="fp32", n_or=N_OR,
                   renorm_every=1, seed=1234 + rank)
     L.set_stream(stream.cuda_stream)
+    L.set_schedule(args.schedule)
+    if args.wave_tuning:
+        L.set_wave_tuning(*args.wave_tuning)
     L.init_hot()
+
+    L_schedule = L.schedule()
 
     def step():
         L.sweep(N_COR)
@@ -391,7 +398,7 @@ def main():
     ms_step = ms / args.steps
     updates_per_step = 3.0 * V * (1 + N_OR) * N_COR
     value = updates_per_step * args.steps * ws / (ms * 1e-3)
-    launches_per_step = N_COR * (6 * (1 + N_OR) + 1) + 1
+    launches_per_step = N_COR * 6 * (1 + N_OR) + 1  # re-projection is fused into the last pass
 
     # ---- dominant kernel: the over-relaxation phase, timed live ----------
     # one qcd_overrelax pass = 6 launches of the OR phase kernel
@@ -405,6 +412,9 @@ def main():
     L.close()
     L2h = q.Lattice(LT, LX, LY, BETA, algo="hb", boundary="pmc", precision="fp32", n_or=0, seed=99)
     L2h.set_stream(stream.cuda_stream)
+    L2h.set_schedule(args.schedule)
+    if args.wave_tuning:
+        L2h.set_wave_tuning(*args.wave_tuning)
     torch.cuda.synchronize()
     L2h.init_hot()
     b0.record(stream)
@@ -500,7 +510,8 @@ def main():
                     "h2d_bytes_per_step": V * 12 * 8 / args.steps, "d2h_bytes_per_step": 16,
                     "note": "one AoS FP64 configuration uploaded from pinned host memory per timed run "
                             "(amortised over the steps); one (energy, plaquette) readback per step"},
-            "gpu_launches": launches_per_step * args.steps,
+            "gpu_launches": launches_per_step * args.steps if L_schedule == "phases" else None,
+            "schedule": L_schedule,
             "batched": batched,
             "clocks": clk.summary(),
         }

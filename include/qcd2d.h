@@ -171,6 +171,19 @@ int qcd_get_schedule(const qcd_lattice* h);
    ready tasks and the live slices).  Defaults: 256 sites, as many passes as
    keep the live slices within ~64 MB, 1 front. */
 int qcd_set_wave_tuning(qcd_lattice* h, int chunk_sites, int passes_per_launch, int fronts);
+/* Autotuner.  Times per-phase launches and the wavefront (task sizes 256 /
+   512 / 1024 sites, 1..32 fronts whose live slices fit in L2, 1 or the
+   largest chain of passes) for sweeps_per_trial sweeps each (0: 2) on this
+   lattice, then restores the lattice's links, streams and counters exactly
+   and keeps the fastest schedule.  The choice is cached per (extents,
+   precision, algorithm, boundary, n_or) for the life of the process, so later
+   handles of the same shape reuse it without timing. */
+typedef struct qcd_tuning {
+  int schedule;           /* QCD_SCHED_PHASES or QCD_SCHED_WAVEFRONT */
+  int chunk_sites, passes_per_launch, fronts;
+  double ms_per_sweep;    /* measured time of the chosen candidate */
+} qcd_tuning;
+int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen);
 /* Host-only planner of the wavefront (no GPU): for a program of n_phases
    phases (mu[n] in {0 y, 1 x, 2 t}, par[n] in {0, 1}) writes each phase's
    seam slice, start step and, in need[o*n_phases + n] (o = 0, 1, 2 for slice

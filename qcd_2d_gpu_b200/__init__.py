@@ -76,6 +76,18 @@ class Params(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    """qcd_tuning (include/qcd2d.h)."""
+
+    _fields_ = [
+        ("schedule", ctypes.c_int),
+        ("chunk_sites", ctypes.c_int),
+        ("passes_per_launch", ctypes.c_int),
+        ("fronts", ctypes.c_int),
+        ("ms_per_sweep", ctypes.c_double),
+    ]
+
+
 class Replica(ctypes.Structure):
     """qcd_replica (include/qcd2d.h)."""
 
@@ -144,6 +156,7 @@ _SIGS = {
     "qcd_wave_plan": (_I, [_P, _P, _I, _P, _P, _P]),
     "qcd_wave_selftest_timeout": (_I, [_P]),
     "qcd_set_wave_tuning": (_I, [_P, _I, _I, _I]),
+    "qcd_autotune": (_I, [_P, _I, ctypes.POINTER(Tuning)]),
     "qcd_batch_create": (_I, [_P, _I, ctypes.POINTER(Params), ctypes.POINTER(_P)]),
     "qcd_batch_destroy": (_I, [_P]),
     "qcd_batch_set_stream": (_I, [_P, _P]),
@@ -272,6 +285,14 @@ class Lattice:
     def set_wave_tuning(self, chunk_sites: int = 0, passes_per_launch: int = 0, fronts: int = 0) -> None:
         self._check(self._lib.qcd_set_wave_tuning(self._h, chunk_sites, passes_per_launch, fronts),
                     "set_wave_tuning")
+
+    def autotune(self, sweeps_per_trial: int = 0) -> dict:
+        """Pick the fastest schedule for this lattice (state is preserved)."""
+        t = Tuning()
+        self._check(self._lib.qcd_autotune(self._h, sweeps_per_trial, ctypes.byref(t)), "autotune")
+        return {"schedule": {SCHED_PHASES: "phases", SCHED_WAVEFRONT: "wavefront"}[t.schedule],
+                "chunk_sites": t.chunk_sites, "passes_per_launch": t.passes_per_launch, "fronts": t.fronts,
+                "ms_per_sweep": t.ms_per_sweep}
 
     def wave_selftest_timeout(self) -> int:
         """Run the bounded-wait self-test; returns the status (expected -5)."""

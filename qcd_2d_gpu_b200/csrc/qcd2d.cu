@@ -10,6 +10,7 @@
 #include <string.h>
 #include <mutex>
 #include <new>
+#include <vector>
 #include "kernels.cuh"
 #include "qcd2d.h"
 #include "wave.cuh"
@@ -774,6 +775,118 @@ int qcd_set_wave_tuning(qcd_lattice* h, int chunk_sites, int passes_per_launch, 
   if (passes_per_launch) h->wave_chain = passes_per_launch;
   if (fronts) h->wave_fronts = fronts;
   return QCD_OK;
+}
+
+// ------------------------------------------------------------- autotune --
+namespace {
+
+struct TuneKey {
+  int lt, lx, ly, prec, algo, bc, n_or;
+  bool operator==(const TuneKey& o) const {
+    return lt == o.lt && lx == o.lx && ly == o.ly && prec == o.prec && algo == o.algo && bc == o.bc && n_or == o.n_or;
+  }
+};
+struct TuneChoice {
+  TuneKey key;
+  qcd_tuning t;
+};
+std::mutex g_tune_mu;
+std::vector<TuneChoice> g_tune_cache;
+
+int apply_tuning(qcd_lattice* h, const qcd_tuning& t) {
+  int rc = qcd_set_schedule(h, t.schedule);
+  if (rc == QCD_OK && t.schedule == QCD_SCHED_WAVEFRONT)
+    rc = qcd_set_wave_tuning(h, t.chunk_sites, t.passes_per_launch, t.fronts);
+  return rc;
+}
+
+}  // namespace
+
+int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
+  if (!h || sweeps_per_trial < 0) return QCD_ERR_INVALID;
+  const TuneKey key{h->p.lt, h->p.lx, h->p.ly, h->p.precision, h->p.algo, h->p.boundary, h->p.n_or};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    for (const TuneChoice& c : g_tune_cache)
+      if (c.key == key) {
+        if (chosen) *chosen = c.t;
+        return apply_tuning(h, c.t);
+      }
+  }
+  if (sweeps_per_trial == 0) sweeps_per_trial = 2;
+  // candidates: per-phase launches, and the wavefront with the task sizes,
+  // fronts and chain lengths whose live slices fit in L2
+  std::vector<qcd_tuning> cand;
+  cand.push_back(qcd_tuning{QCD_SCHED_PHASES, 0, 0, 0, 0.0});
+  int rc = wave_setup(h);
+  if (rc) return rc;
+  const double slice_bytes = (double)h->g.slice * (6.0 * (h->p.precision == QCD_PREC_FP64 ? 32.0 : 16.0) + 24.0);
+  const int max_chain = h->wave_chain;
+  for (int chunk : {256, 512, 1024})
+    for (int fronts : {1, 2, 4, 8, 16, 32})
+      for (int passes : {1, max_chain}) {
+        if (h->g.lt % fronts || h->g.lt / fronts < 2) continue;
+        if (passes != 1 && passes == max_chain && max_chain == 1) continue;
+        if (fronts > 1 && fronts * wave_window(passes) * slice_bytes > 100.0 * 1024 * 1024) continue;
+        cand.push_back(qcd_tuning{QCD_SCHED_WAVEFRONT, chunk, passes, fronts, 0.0});
+      }
+  // the trials advance the lattice: save links, streams and counters, restore after
+  const size_t rng_bytes = 6 * (size_t)h->g.vh * sizeof(uint32_t);
+  void *links_save = nullptr, *links2_save = nullptr, *rng_save = nullptr, *acc_save = nullptr;
+  const size_t lb = h->p.precision == QCD_PREC_FP64 ? h->link_bytes / 2 : h->link_bytes;
+  void* lp = h->p.precision == QCD_PREC_FP64 ? (void*)h->lo : (void*)h->q32;
+  CUDA_OR_FAIL(h, cudaMalloc(&links_save, lb));
+  if (h->p.precision == QCD_PREC_FP64) CUDA_OR_FAIL(h, cudaMalloc(&links2_save, lb));
+  CUDA_OR_FAIL(h, cudaMalloc(&rng_save, rng_bytes));
+  if (h->accept) CUDA_OR_FAIL(h, cudaMalloc(&acc_save, (size_t)h->V * sizeof(int)));
+  CUDA_OR_FAIL(h, cudaMemcpyAsync(links_save, lp, lb, cudaMemcpyDeviceToDevice, h->stream));
+  if (links2_save) CUDA_OR_FAIL(h, cudaMemcpyAsync(links2_save, h->hi, lb, cudaMemcpyDeviceToDevice, h->stream));
+  CUDA_OR_FAIL(h, cudaMemcpyAsync(rng_save, h->rng, rng_bytes, cudaMemcpyDeviceToDevice, h->stream));
+  if (acc_save)
+    CUDA_OR_FAIL(h, cudaMemcpyAsync(acc_save, h->accept, (size_t)h->V * sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
+  const long long passes_save = h->unit_passes, sweeps_save = h->sweeps_done;
+  const int sched_save = h->sched, chunk_save = h->wave_chunk, chain_save = h->wave_chain, fronts_save = h->wave_fronts;
+  cudaEvent_t e0, e1;
+  CUDA_OR_FAIL(h, cudaEventCreate(&e0));
+  CUDA_OR_FAIL(h, cudaEventCreate(&e1));
+  int best = 0;
+  for (size_t i = 0; i < cand.size() && rc == QCD_OK; i++) {
+    rc = apply_tuning(h, cand[i]);
+    if (rc == QCD_OK) rc = qcd_sweep(h, 1);  // warm-up (task tables, first launches)
+    if (rc == QCD_OK) rc = cudaEventRecord(e0, h->stream) == cudaSuccess ? QCD_OK : QCD_ERR_CUDA;
+    if (rc == QCD_OK) rc = qcd_sweep(h, sweeps_per_trial);
+    if (rc == QCD_OK) rc = cudaEventRecord(e1, h->stream) == cudaSuccess ? QCD_OK : QCD_ERR_CUDA;
+    if (rc == QCD_OK) rc = check_device_error(h);
+    float ms = 0;
+    if (rc == QCD_OK) rc = cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess ? QCD_OK : QCD_ERR_CUDA;
+    cand[i].ms_per_sweep = ms / sweeps_per_trial;
+    if (rc == QCD_OK && cand[i].ms_per_sweep < cand[best].ms_per_sweep) best = (int)i;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // restore the lattice as it was
+  cudaMemcpyAsync(lp, links_save, lb, cudaMemcpyDeviceToDevice, h->stream);
+  if (links2_save) cudaMemcpyAsync(h->hi, links2_save, lb, cudaMemcpyDeviceToDevice, h->stream);
+  cudaMemcpyAsync(h->rng, rng_save, rng_bytes, cudaMemcpyDeviceToDevice, h->stream);
+  if (acc_save) cudaMemcpyAsync(h->accept, acc_save, (size_t)h->V * sizeof(int), cudaMemcpyDeviceToDevice, h->stream);
+  cudaStreamSynchronize(h->stream);
+  cudaFree(links_save);
+  cudaFree(links2_save);
+  cudaFree(rng_save);
+  cudaFree(acc_save);
+  h->unit_passes = passes_save;
+  h->sweeps_done = sweeps_save;
+  h->sched = sched_save;
+  h->wave_chunk = chunk_save;
+  h->wave_chain = chain_save;
+  h->wave_fronts = fronts_save;
+  if (rc) return rc;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache.push_back(TuneChoice{key, cand[best]});
+  }
+  if (chosen) *chosen = cand[best];
+  return apply_tuning(h, cand[best]);
 }
 
 int qcd_wave_plan(const int* mu, const int* par, int n_phases, int* seam, int* start, int* need) {

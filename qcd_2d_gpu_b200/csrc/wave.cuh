@@ -118,12 +118,18 @@ __device__ __forceinline__ void wave_site(const Links32T<true>& L, const RngStor
 // update kind (heat-bath or Metropolis); over-relaxation phases are KIND_OR.
 template <class LinksT, int BC, int SK>
 __global__ void __launch_bounds__(kBlock, 5) wave(LinksT L, RngStoreT<true> R, Geo g, PhaseArgs a,
-                                               WaveSched S, WaveCtl c) {
+                                                  WaveSched S, WaveCtl c) {
   __shared__ int sh_ok, sh_n, sh_t, sh_chunk;
+  // Thread 0 keeps one ticket in hand: the atomic for the next ticket is
+  // issued before the CTA computes the current task, so its latency hides
+  // behind the work.  A CTA never waits while holding an unstarted ticket
+  // that others need: the current task's waits are over before the next
+  // ticket is drawn, so the current task finishes and the next one starts.
+  unsigned int tk = 0;
+  if (threadIdx.x == 0) tk = atomicAdd(c.queue, 1u);
   for (;;) {
     if (threadIdx.x == 0) {
       int ok = 0, n = 0, t = 0, chunk = 0;
-      const unsigned int tk = atomicAdd(c.queue, 1u);
       if (tk < S.n_tasks && !*(volatile int*)c.abort) {
         const unsigned int w = __ldg(c.tasks + tk);
         n = (int)(w & 31u);
@@ -160,6 +166,7 @@ __global__ void __launch_bounds__(kBlock, 5) wave(LinksT L, RngStoreT<true> R, G
             if (it > 32) __nanosleep(64);
           }
         }
+        if (ok) tk = atomicAdd(c.queue, 1u);  // next ticket, in flight during the work
       }
       sh_ok = ok;
       sh_n = n;

@@ -75,3 +75,22 @@ def test_bounded_wait_reports_timeout_and_context_survives():
     e, p = L.measure()
     assert 0.0 < p < 1.0
     L.close()
+
+
+def test_autotune_keeps_the_lattice_and_picks_a_schedule():
+    kw = dict(boundary=2, precision="fp32", n_or=1, renorm_every=1, seed=8)
+    a = q.Lattice(24, 16, 32, 7.0, **kw)
+    b = q.Lattice(24, 16, 32, 7.0, **kw)
+    for L in (a, b):
+        L.init_hot()
+        L.sweep(2)
+    t = a.autotune(2)
+    assert t["schedule"] in ("phases", "wavefront") and t["ms_per_sweep"] > 0
+    # tuning left no trace: both lattices continue identically (all schedules are bit-identical)
+    a.sweep(3)
+    b.sweep(3)
+    assert np.array_equal(a.store_config(), b.store_config())
+    assert np.array_equal(a.accept_counts(), b.accept_counts())
+    # a second handle of the same shape reuses the cached choice
+    c = q.Lattice(24, 16, 32, 7.0, **kw)
+    assert c.autotune(2) == t
