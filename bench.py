@@ -113,11 +113,16 @@ def c4_replicas():
     return reps
 
 
-def run_batch_c4(q, torch, stream):
+def run_batch_c4(q, torch, stream, rank=0, world=1, dist=None):
     """Batched replicas: the 96 lattices in shared launches, FP32 heat-bath,
     a measurement every sweep, the interval replayed as a CUDA graph; timed
-    from the seeding of the streams to the last measurement."""
-    reps = c4_replicas()
+    from the seeding of the streams to the last measurement.  Under torchrun
+    the replicas are shared out between the ranks (no collective on the data
+    path); the rate is all replicas / the slowest rank's time."""
+    from qcd_2d_gpu_b200.replicas import job_rate, shard
+
+    all_reps = c4_replicas()
+    reps = shard(all_reps, rank, world)
     sites = sum(r["lt"] * r["lx"] * r["ly"] for r in reps)
     B = q.Batch(reps, algo="hb", precision="fp32", renorm_every=1)
     B.set_stream(stream.cuda_stream)
@@ -135,10 +140,13 @@ def run_batch_c4(q, torch, stream):
     ms = e0.elapsed_time(e1)
     assert B.measured() == C4_SWEEPS
     B.close()
+    rate, ms_max = job_rate(float(len(reps)), ms, dist, device="cuda")
+    ups, _ = job_rate(3.0 * sites * C4_SWEEPS, ms, dist, device="cuda")
     return {"workload": f"96 replicas (Nt=Nx in 8..64, Ny in 8..128, beta in [3,12], bc r mod 3, half hot), "
-                        f"FP32 heat-bath, {C4_SWEEPS} sweeps with a measurement each, CUDA graph",
-            "replicas_per_s": len(reps) / (ms * 1e-3), "link_updates_per_s": 3.0 * sites * C4_SWEEPS / (ms * 1e-3),
-            "ms": ms, "sites": sites}
+                        f"FP32 heat-bath, {C4_SWEEPS} sweeps with a measurement each, CUDA graph"
+                        + (f", shared out over {world} ranks" if world > 1 else ""),
+            "replicas_per_s": rate, "link_updates_per_s": ups, "ms": ms_max,
+            "sites": sum(r["lt"] * r["lx"] * r["ly"] for r in all_reps)}
 
 
 def reference_accuracy(args):
@@ -474,7 +482,7 @@ def main():
     e2e_value = updates_per_step * args.steps * ws / (e2e_ms * 1e-3)
     E.close()
 
-    batched = run_batch_c4(q, torch, stream) if not args.no_batch else None
+    batched = run_batch_c4(q, torch, stream, rank, ws, dist) if not args.no_batch else None
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

@@ -195,6 +195,13 @@ int qcd_wave_plan(const int* mu, const int* par, int n_phases, int* seam, int* s
    updated: re-initialise the lattice afterwards). */
 int qcd_wave_selftest_timeout(qcd_lattice* h);
 
+/* Random-generator checkpoint: the 6 x V/2 u32 words of the MRG32k3a
+   streams.  No counterpart in the reference (a restart re-seeds with
+   time(NULL), kernel.cu:79); with it a run resumed from a Config_ file
+   continues the chain bit for bit. */
+int qcd_store_rng(qcd_lattice* h, uint32_t* host_out);
+int qcd_load_rng(qcd_lattice* h, const uint32_t* host_in);
+
 /* Lattice facts. */
 long long qcd_volume(const qcd_lattice* h);
 int qcd_get_params(const qcd_lattice* h, qcd_params* out);

@@ -156,6 +156,8 @@ _SIGS = {
     "qcd_wave_plan": (_I, [_P, _P, _I, _P, _P, _P]),
     "qcd_wave_selftest_timeout": (_I, [_P]),
     "qcd_set_wave_tuning": (_I, [_P, _I, _I, _I]),
+    "qcd_store_rng": (_I, [_P, _P]),
+    "qcd_load_rng": (_I, [_P, _P]),
     "qcd_autotune": (_I, [_P, _I, ctypes.POINTER(Tuning)]),
     "qcd_batch_create": (_I, [_P, _I, ctypes.POINTER(Params), ctypes.POINTER(_P)]),
     "qcd_batch_destroy": (_I, [_P]),
@@ -341,6 +343,17 @@ class Lattice:
         if a.size != self.V * 12:
             raise ValueError(f"configuration has {a.size} doubles, expected {self.V * 12}")
         self._check(self._lib.qcd_load_config(self._h, _ptr(a)), "load_config")
+
+    def store_rng(self) -> np.ndarray:
+        out = np.empty(6 * (self.V // 2), dtype=np.uint32)
+        self._check(self._lib.qcd_store_rng(self._h, _ptr(out)), "store_rng")
+        return out
+
+    def load_rng(self, words: np.ndarray) -> None:
+        a = np.ascontiguousarray(words, dtype=np.uint32)
+        if a.size != 6 * (self.V // 2):
+            raise ValueError("generator state has the wrong size")
+        self._check(self._lib.qcd_load_rng(self._h, _ptr(a)), "load_rng")
 
     def accept_counts(self) -> np.ndarray:
         out = np.empty(self.V, dtype=np.int32)

@@ -1008,6 +1008,25 @@ int qcd_check_unitarity(qcd_lattice* h, double tol, double* mean_det) {
   return QCD_OK;
 }
 
+// The six u32 words of each of the V/2 MRG32k3a streams, plane by plane
+// (word j of stream id at [j * V/2 + id]).  The reference keeps no generator
+// state across runs (a restart re-seeds, kernel.cu:79); saving it next to the
+// configuration makes a resumed run continue the exact same chain.
+int qcd_store_rng(qcd_lattice* h, uint32_t* host_out) {
+  if (!h || !host_out) return QCD_ERR_INVALID;
+  CUDA_OR_FAIL(h, cudaMemcpyAsync(host_out, h->rng, 6 * (size_t)h->g.vh * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                  h->stream));
+  return check_device_error(h);
+}
+
+int qcd_load_rng(qcd_lattice* h, const uint32_t* host_in) {
+  if (!h || !host_in) return QCD_ERR_INVALID;
+  CUDA_OR_FAIL(h, cudaMemcpyAsync(h->rng, host_in, 6 * (size_t)h->g.vh * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                  h->stream));
+  CUDA_OR_FAIL(h, cudaStreamSynchronize(h->stream));
+  return QCD_OK;
+}
+
 long long qcd_volume(const qcd_lattice* h) { return h ? h->V : 0; }
 
 int qcd_get_params(const qcd_lattice* h, qcd_params* out) {

@@ -13,6 +13,8 @@
  *         [--outdir DIR]
  *   extensions: [--precision fp64|fp32] [--n-or K] [--renorm-every K]
  *               [--schedule auto|phases|wavefront] [--report]
+ *               [--rng-state 1: save the generator state next to the Config_
+ *                files and resume from it, so a restart continues the chain]
  *
  * With --precision fp64 (the default) the update arithmetic and the random
  * draws are the reference's, so for the same seed the files match a run of
@@ -35,7 +37,7 @@ typedef struct {
   int have_seed;
   char nsave[16], nconfr[16], nconfs[16];
   const char* outdir;
-  int precision, n_or, renorm_every, schedule, report;
+  int precision, n_or, renorm_every, schedule, report, rng_state;
 } knobs;
 
 static void defaults(knobs* k) {  // kernel.cu:11-46
@@ -74,7 +76,7 @@ static int usage(void) {
           "             [--N-block N] [--Nblock-term N] [--Nsave N] [--N-cor N] [--epsilon E] [--upd N]\n"
           "             [--W N] [--seed S] [--nsave S] [--nconfr S] [--nconfs S] [--outdir DIR]\n"
           "             [--precision fp64|fp32] [--n-or K] [--renorm-every K]\n"
-          "             [--schedule auto|phases|wavefront] [--report]\n");
+          "             [--schedule auto|phases|wavefront] [--report] [--rng-state 0|1]\n");
   return 2;
 }
 
@@ -112,6 +114,7 @@ static int parse(int argc, char** argv, knobs* k) {
     INT_OPT("--W", W)
     INT_OPT("--n-or", n_or)
     INT_OPT("--renorm-every", renorm_every)
+    INT_OPT("--rng-state", rng_state)
     else if (!strcmp(a, "--beta")) k->beta = atof(v);
     else if (!strcmp(a, "--epsilon")) k->epsilon = atof(v);
     else if (!strcmp(a, "--seed")) {
@@ -138,6 +141,13 @@ static int parse(int argc, char** argv, knobs* k) {
       k->readconf > 2)
     return usage();
   return 0;
+}
+
+/* Config_<...>_rng.bin: the 6 x V/2 u32 generator words (qcd_store_rng) */
+static void rng_path(char* out, size_t cap, const char* dir, const refio_lattice* l, const char* bound,
+                     const char* n) {
+  snprintf(out, cap, "%s%sConfig_%d_%d_%d_B_%.2lf_%s_%s_rng.bin", dir, dir[0] ? "/" : "", l->t, l->x, l->y,
+           (double)l->beta, bound, n);
 }
 
 #define CHECK(call)                                                                       \
@@ -209,6 +219,20 @@ int main(int argc, char** argv) {
     else CHECK(qcd_init_cold(h));
   } else {
     CHECK(qcd_load_config(h, phi));
+    if (k.rng_state) {  // resume the generator chain saved with the configuration
+      char rp[1024];
+      rng_path(rp, sizeof(rp), k.outdir, &l, bound, k.nconfr);
+      const size_t nw = 6 * (size_t)(l.V / 2);
+      unsigned int* w = (unsigned int*)malloc(nw * sizeof(unsigned int));
+      FILE* f = fopen(rp, "rb");
+      if (!w || !f || fread(w, sizeof(unsigned int), nw, f) != nw) {
+        printf("Error reading %s\n", rp);
+        exit(1);
+      }
+      fclose(f);
+      CHECK(qcd_load_rng(h, w));
+      free(w);
+    }
   }
   CHECK(qcd_store_config(h, phi));
   refio_print_det(phi, &l);
@@ -236,6 +260,21 @@ int main(int argc, char** argv) {
     if (k.sconf == 0) {
       CHECK(qcd_store_config(h, phi));
       if (refio_save_conf(k.outdir, phi, &l, Nterms, inits, bound, k.nconfs)) exit(1);
+      if (k.rng_state) {
+        char rp[1024];
+        rng_path(rp, sizeof(rp), k.outdir, &l, bound, k.nconfs);
+        const size_t nw = 6 * (size_t)(l.V / 2);
+        unsigned int* w = (unsigned int*)malloc(nw * sizeof(unsigned int));
+        if (!w) exit(1);
+        CHECK(qcd_store_rng(h, w));
+        FILE* f = fopen(rp, "wb");
+        if (!f || fwrite(w, sizeof(unsigned int), nw, f) != nw) {
+          printf("Error creating the file");
+          exit(1);
+        }
+        fclose(f);
+        free(w);
+      }
     }
   }
   CHECK(qcd_store_config(h, phi));

@@ -128,3 +128,21 @@ def test_fp32_driver_run_with_report(tmp_path):
     assert b.returncode == 0, b.stderr
     assert "report Plaquette" in b.stdout
     assert any(n.startswith("Check_16_16_16_B_6.00_pmc_1") for n in os.listdir(tmp_path))
+
+
+def test_driver_resume_with_generator_state(tmp_path):
+    from qcd_2d_gpu_b200.build import build_driver
+
+    build_driver()
+    common = ["--dt", 8, "--dx", 8, "--dy", 8, "--beta", 6, "--boundary", 0, "--N", 12, "--N-cor", 2, "--W", 3,
+              "--Nsave", 1, "--seed", 5, "--rng-state", 1, "--outdir", str(tmp_path)]
+    a = subprocess.run([DRIVER, *map(str, common + ["--N-term", 10])], capture_output=True, text=True, timeout=300)
+    assert a.returncode == 0, a.stderr
+    assert any(n.endswith("_rng.bin") for n in os.listdir(tmp_path))
+    first = (tmp_path / "Check_8_8_8_B_6.00_per_1.txt").read_text()
+    b = subprocess.run([DRIVER, *map(str, common + ["--readconf", 2, "--nsave", 2])], capture_output=True, text=True,
+                       timeout=300)
+    assert b.returncode == 0, b.stderr + b.stdout
+    # resumed from the saved links and generator words: the same measurement chain
+    second = (tmp_path / "Check_8_8_8_B_6.00_per_2.txt").read_text()
+    assert first.splitlines()[2:] == second.splitlines()[2:]

@@ -199,3 +199,19 @@ def test_accept_counts_heatbath_pcc():
             assert acc[par, i] == (3 if y == 0 else 9)
     L.accept_reset()
     assert not L.accept_counts().any()
+
+
+def test_generator_checkpoint_resumes_the_chain_exactly():
+    kw = dict(boundary=1, precision="fp64", seed=21)
+    a = q.Lattice(8, 8, 12, 6.5, **kw)
+    a.init_hot()
+    a.sweep(10)
+    b = q.Lattice(8, 8, 12, 6.5, **kw)
+    b.init_hot()
+    b.sweep(5)
+    cfg, rng = b.store_config(), b.store_rng()
+    c = q.Lattice(8, 8, 12, 6.5, **dict(kw, seed=999))  # seeded differently on purpose
+    c.load_config(cfg)
+    c.load_rng(rng)
+    c.sweep(5)
+    assert np.array_equal(c.store_config(), a.store_config())
