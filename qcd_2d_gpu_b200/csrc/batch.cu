@@ -42,6 +42,7 @@ struct Replica {
 
 struct BatchView {
   const Replica* rep;
+  const int* cta_rep;  // replica of every CTA of a batched launch
   int n;
   float4* q32;
   double2* lo;
@@ -49,17 +50,7 @@ struct BatchView {
   uint32_t* rng;
 };
 
-__device__ __forceinline__ int replica_of(const BatchView& B, int cta) {
-  int lo = 0, hi = B.n - 1;
-  while (lo < hi) {  // last replica with cta_begin <= cta
-    int mid = (lo + hi + 1) >> 1;
-    if (B.rep[mid].cta_begin <= cta)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  return lo;
-}
+__device__ __forceinline__ int replica_of(const BatchView& B, int cta) { return __ldg(B.cta_rep + cta); }
 
 struct BatchArgs {
   float eps;
@@ -251,6 +242,7 @@ struct qcd_batch {
   int ctas = 0;
   cudaStream_t own = nullptr, stream = nullptr;
   Replica* rep_dev = nullptr;
+  int* cta_rep = nullptr;
   float4* q32 = nullptr;
   double2* lo = nullptr;
   double2* hi = nullptr;
@@ -292,7 +284,7 @@ int bfail(qcd_batch* b, int code, const char* fmt, ...) {
     }                                                                                               \
   } while (0)
 
-BatchView view(const qcd_batch* b) { return BatchView{b->rep_dev, b->n, b->q32, b->lo, b->hi, b->rng}; }
+BatchView view(const qcd_batch* b) { return BatchView{b->rep_dev, b->cta_rep, b->n, b->q32, b->lo, b->hi, b->rng}; }
 
 bool fp64(const qcd_batch* b) { return b->common.precision == QCD_PREC_FP64; }
 
@@ -344,6 +336,7 @@ bool renorm_due(const qcd_batch* b, long long sweep_index) {
 void release(qcd_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   cudaFree(b->rep_dev);
+  cudaFree(b->cta_rep);
   cudaFree(b->q32);
   cudaFree(b->lo);
   cudaFree(b->hi);
@@ -419,6 +412,16 @@ int qcd_batch_create(const qcd_replica* r, int n, const qcd_params* common, qcd_
   if (rc == QCD_OK) step(cudaMalloc(&b->rep_dev, n * sizeof(Replica)), "cudaMalloc(replicas)");
   if (rc == QCD_OK)
     step(cudaMemcpy(b->rep_dev, b->rep.data(), n * sizeof(Replica), cudaMemcpyHostToDevice), "replica table");
+  if (rc == QCD_OK) {
+    std::vector<int> owner((size_t)cta);
+    for (int i = 0; i < n; i++) {
+      const int end = i + 1 < n ? b->rep[i + 1].cta_begin : cta;
+      for (int c = b->rep[i].cta_begin; c < end; c++) owner[c] = i;
+    }
+    step(cudaMalloc(&b->cta_rep, (size_t)cta * sizeof(int)), "cudaMalloc(cta table)");
+    if (rc == QCD_OK)
+      step(cudaMemcpy(b->cta_rep, owner.data(), (size_t)cta * sizeof(int), cudaMemcpyHostToDevice), "cta table");
+  }
   if (common->precision == QCD_PREC_FP64) {
     if (rc == QCD_OK) step(cudaMalloc(&b->lo, link_off * sizeof(double2)), "cudaMalloc(links)");
     if (rc == QCD_OK) step(cudaMalloc(&b->hi, link_off * sizeof(double2)), "cudaMalloc(links)");

@@ -163,6 +163,15 @@ __device__ __forceinline__ Quat<double> ld64<Links32>(const Links32& links, int 
   return Quat<double>{u.w, u.x, u.y, u.z};
 }
 
+// FP32 links: the three products in FP32 (the link's own precision), the
+// result handed to the FP64 sums
+__device__ __forceinline__ double plaq(const Links32& links, int mu, int nu, int p, int id, int omu, int onu) {
+  Quat<float> A = q_mul(links.ld(mu, p, id), links.ld(nu, p ^ 1, id + omu));
+  Quat<float> B = q_mul_bd(A, links.ld(mu, p ^ 1, id + onu));
+  A = q_mul_bd(B, links.ld(nu, p, id));
+  return 1.0 - (double)A.w;
+}
+
 template <class L>
 __device__ __forceinline__ double plaq(const L& links, int mu, int nu, int p, int id, int omu,
                                        int onu) {

@@ -34,7 +34,13 @@ def test_noalloc_matches_measure_on_two_calls(bc, precision):
     L.sweep(3)
     phi = torch.empty(lt * lx * ly * 12, dtype=torch.float64, device="cuda")
     assert lib.qcd_store_config_device(L.handle, _dev_ptr(phi)) == 0
-    e_ref, p_ref = L.measure()  # synchronises the handle's stream
+    L.measure()  # synchronises the handle's stream
+    # the existing entry point on the same FP64 links (an FP32 lattice's links
+    # are exact in FP64): qcd_measure of an FP64 handle holding them
+    R = q.Lattice(lt, lx, ly, 7.0, boundary=bc, precision="fp64", seed=1)
+    assert lib.qcd_load_config_device(R.handle, _dev_ptr(phi)) == 0
+    e_ref, p_ref = R.measure()
+    R.close()
     torch.cuda.synchronize()
     out = torch.empty(2, dtype=torch.float64, device="cuda")
     for _ in range(2):  # the scratch keeps the previous call's contents
