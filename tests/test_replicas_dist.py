@@ -41,7 +41,7 @@ def test_job_rate_two_gloo_ranks():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         port = s.getsockname()[1]
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()  # no fork: the parent may hold CUDA state
     mp.spawn(_worker, args=(2, port, out), nprocs=2, join=True)
     # 10 replicas in total, the slowest rank took 2 ms
     assert out[0] == out[1] == (10 / 2e-3, 2.0)
