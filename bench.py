@@ -406,10 +406,14 @@ def main():
     ms_step = ms / args.steps
     updates_per_step = 3.0 * V * (1 + N_OR) * N_COR
     value = updates_per_step * args.steps * ws / (ms * 1e-3)
-    launches_per_step = N_COR * 6 * (1 + N_OR) + 1  # re-projection is fused into the last pass
+    # launches of one pass: six phase kernels (the wavefront runs passes in
+    # persistent launches); the re-projection rides on the last pass, the
+    # measurement is one launch
+    per_pass = {"phases": 6}.get(L_schedule)
+    launches_per_step = N_COR * per_pass * (1 + N_OR) + 1 if per_pass else None
 
-    # ---- dominant kernel: the over-relaxation phase, timed live ----------
-    # one qcd_overrelax pass = 6 launches of the OR phase kernel
+    # ---- dominant kernel: the over-relaxation pass, timed live -----------
+    # one qcd_overrelax pass = 6 phase launches
     reps = 5
     a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a0.record(stream)
@@ -429,18 +433,24 @@ def main():
     L2h.sweep(reps)
     b1.record(stream)
     torch.cuda.synchronize()
-    or_launch_ms = a0.elapsed_time(a1) / (6 * reps)
-    hb_launch_ms = b0.elapsed_time(b1) / (6 * reps)
+    n_launch = per_pass or 6
+    or_pass_ms = a0.elapsed_time(a1) / reps
+    hb_pass_ms = b0.elapsed_time(b1) / reps
+    or_launch_ms = or_pass_ms / n_launch
+    hb_launch_ms = hb_pass_ms / n_launch
     L2h.close()
-    vh = V // 2
-    or_bytes = 32.0 * vh  # strict: each FP32 link read once and written once
-    hb_bytes = 40.0 * vh  # + 2 x 24 B MRG32k3a state per 6 updates
+    # strict algorithmic bytes: each FP32 link read once and written once per
+    # pass (32 B per update), plus for the heat-bath 2 x 24 B of MRG32k3a state
+    # per 6 updates (40 B per update); a pass is 3V updates
+    or_bytes = 32.0 * 3 * V / n_launch
+    hb_bytes = 40.0 * 3 * V / n_launch
     hbm, peak_kind = peaks()
     or_gbs = or_bytes / (or_launch_ms * 1e-3) / 1e9
-    roofline = {"kernel": "phase32<OR> (over-relaxation phase)", "bound": "hbm", "achieved": or_gbs,
+    roofline = {"kernel": "phase32<mu, par, PMC, OR> (over-relaxation phase)", "bound": "hbm", "achieved": or_gbs,
                 "peak": hbm, "unit": "GB/s", "frac": or_gbs / hbm, "peak_source": peak_kind,
                 "traffic": None, "algorithmic_bytes_per_launch": or_bytes, "launch_ms": or_launch_ms,
-                "heatbath_phase": {"launch_ms": hb_launch_ms, "achieved": hb_bytes / (hb_launch_ms * 1e-3) / 1e9}}
+                "launches_per_pass": n_launch,
+                "heatbath": {"launch_ms": hb_launch_ms, "achieved": hb_bytes / (hb_launch_ms * 1e-3) / 1e9}}
     traffic_file = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(traffic_file):
         try:
@@ -509,16 +519,16 @@ def main():
                        "n_cor": N_COR, "beta": BETA,
                        "l2": f"inputs larger than L2 ({V * 48 / 1e9:.2f} GB FP32 link store)",
                        "parallelism": f"replicas x{ws}"},
-            # one heat-bath pass alone (6 phase launches, timed live above): the
-            # rate comparable with the reference's heat-bath-only sweep
-            "heatbath_pass_link_updates_per_s": 3.0 * V / (6 * hb_launch_ms * 1e-3),
+            # one heat-bath pass alone (timed live above): the rate comparable
+            # with the reference's heat-bath-only sweep
+            "heatbath_pass_link_updates_per_s": 3.0 * V / (hb_pass_ms * 1e-3),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "link updates/s",
                     "h2d_bytes_per_step": V * 12 * 8 / args.steps, "d2h_bytes_per_step": 16,
                     "note": "one AoS FP64 configuration uploaded from pinned host memory per timed run "
                             "(amortised over the steps); one (energy, plaquette) readback per step"},
-            "gpu_launches": launches_per_step * args.steps if L_schedule == "phases" else None,
+            "gpu_launches": launches_per_step * args.steps if launches_per_step else None,
             "schedule": L_schedule,
             "batched": batched,
             "clocks": clk.summary(),
