@@ -410,7 +410,8 @@ def main():
     # persistent launches); the re-projection rides on the last pass, the
     # measurement is one launch
     per_pass = {"phases": 6}.get(L_schedule)
-    launches_per_step = N_COR * per_pass * (1 + N_OR) + 1 if per_pass else None
+    # + one one-thread launch per heat-bath pass advancing the FP32 draws' counter
+    launches_per_step = N_COR * (per_pass * (1 + N_OR) + 1) + 1 if per_pass else None
 
     # ---- dominant kernel: the over-relaxation pass, timed live -----------
     # one qcd_overrelax pass = 6 phase launches

@@ -195,12 +195,25 @@ int qcd_wave_plan(const int* mu, const int* par, int n_phases, int* seam, int* s
    updated: re-initialise the lattice afterwards). */
 int qcd_wave_selftest_timeout(qcd_lattice* h);
 
-/* Random-generator checkpoint: the 6 x V/2 u32 words of the MRG32k3a
-   streams.  No counterpart in the reference (a restart re-seeds with
+/* Random-generator checkpoint: qcd_rng_words(h) u32 words = the 6 x V/2
+   words of the MRG32k3a streams (plane j of stream id at j * V/2 + id; the
+   FP64 draws and every hot start) followed by the 64-bit drawing-phase
+   counter and the 64-bit key of the FP32 sweep's counter-based draws (low
+   words first).  No counterpart in the reference (a restart re-seeds with
    time(NULL), kernel.cu:79); with it a run resumed from a Config_ file
    continues the chain bit for bit. */
+long long qcd_rng_words(const qcd_lattice* h);
 int qcd_store_rng(qcd_lattice* h, uint32_t* host_out);
 int qcd_load_rng(qcd_lattice* h, const uint32_t* host_in);
+
+/* Philox4x32-10 block (Salmon et al., SC'11) on the host, the generator of
+   the FP32 sweep: out = philox(ctr, key).  The heat-bath or Metropolis update
+   of site id (sublattice index) in drawing phase k (6 per heat-bath or
+   Metropolis pass, counted from the handle's creation) of a lattice with
+   seed s reads blocks ctr = {id, b, k lo, k hi}, b = 0, 1, ..., key = {s lo,
+   s hi}, word by word: float draws are ((w >> 8) + 1) / 2^24, double draws
+   take two words.  Pure host code (no GPU). */
+void qcd_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 
 /* Lattice facts. */
 long long qcd_volume(const qcd_lattice* h);

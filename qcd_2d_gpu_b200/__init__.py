@@ -156,6 +156,8 @@ _SIGS = {
     "qcd_wave_plan": (_I, [_P, _P, _I, _P, _P, _P]),
     "qcd_wave_selftest_timeout": (_I, [_P]),
     "qcd_set_wave_tuning": (_I, [_P, _I, _I, _I]),
+    "qcd_rng_words": (ctypes.c_longlong, [_P]),
+    "qcd_philox4x32": (None, [_P, _P, _P]),
     "qcd_store_rng": (_I, [_P, _P]),
     "qcd_load_rng": (_I, [_P, _P]),
     "qcd_autotune": (_I, [_P, _I, ctypes.POINTER(Tuning)]),
@@ -345,13 +347,14 @@ class Lattice:
         self._check(self._lib.qcd_load_config(self._h, _ptr(a)), "load_config")
 
     def store_rng(self) -> np.ndarray:
-        out = np.empty(6 * (self.V // 2), dtype=np.uint32)
+        """The generator checkpoint (MRG32k3a words + the FP32 draws' counter and key)."""
+        out = np.empty(self._lib.qcd_rng_words(self._h), dtype=np.uint32)
         self._check(self._lib.qcd_store_rng(self._h, _ptr(out)), "store_rng")
         return out
 
     def load_rng(self, words: np.ndarray) -> None:
         a = np.ascontiguousarray(words, dtype=np.uint32)
-        if a.size != 6 * (self.V // 2):
+        if a.size != self._lib.qcd_rng_words(self._h):
             raise ValueError("generator state has the wrong size")
         self._check(self._lib.qcd_load_rng(self._h, _ptr(a)), "load_rng")
 
@@ -468,6 +471,18 @@ def rng_tape(seed: int, first: int, n_streams: int, n_draws: int, lib: ctypes.CD
     if rc != QCD_OK:
         raise QcdError(rc, "qcd_rng_tape")
     return out.reshape(n_streams, n_draws)
+
+
+def philox4x32(ctr, key, lib: ctypes.CDLL | None = None) -> np.ndarray:
+    """One Philox4x32-10 block (the FP32 sweep's generator), computed on the host."""
+    lib = lib or load_library()
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    if c.size != 4 or k.size != 2:
+        raise ValueError("ctr has 4 words, key 2")
+    out = np.empty(4, dtype=np.uint32)
+    lib.qcd_philox4x32(_ptr(c), _ptr(k), _ptr(out))
+    return out
 
 
 def wave_plan(mu, par, lib: ctypes.CDLL | None = None):

@@ -58,6 +58,8 @@ struct BatchArgs {
   int* err;
   int* accept;
   int renorm;
+  const unsigned long long* phase_ptr;  // drawing phases run so far (device word)
+  unsigned int phase_off;               // this phase's offset from it
 };
 
 template <int MU, int PAR, int KIND, bool FP64>
@@ -67,7 +69,10 @@ __global__ void __launch_bounds__(kBlock) batch_phase(BatchView B, BatchArgs a) 
   const int id = (blockIdx.x - R.cta_begin) * kBlock + threadIdx.x;
   if (id >= R.g.vh) return;
   const Nbr n = make_nbr(R.g, id, PAR);
-  PhaseArgs pa{R.beta, a.eps, a.upd, a.err, a.accept ? a.accept + R.site_off : nullptr, a.renorm};
+  // FP32 draws: the replica's seed as key, its stream offset added to the
+  // site index, the batch-wide drawing-phase counter (as for one lattice)
+  PhaseArgs pa{R.beta, a.eps, a.upd, a.err, a.accept ? a.accept + R.site_off : nullptr, a.renorm,
+               R.seed, a.phase_ptr, a.phase_off, (unsigned int)R.stream_off};
   RngStore RS{B.rng + R.rng_off, R.g.vh};
   if (FP64) {
     Links64 L{B.lo + R.link_off, B.hi + R.link_off, R.g.vh};
@@ -247,6 +252,7 @@ struct qcd_batch {
   double2* lo = nullptr;
   double2* hi = nullptr;
   uint32_t* rng = nullptr;
+  unsigned long long* draw_dev = nullptr;  // drawing phases run so far (FP32 draws)
   int* accept = nullptr;
   int* err = nullptr;
   double2* partials = nullptr;
@@ -289,12 +295,17 @@ BatchView view(const qcd_batch* b) { return BatchView{b->rep_dev, b->cta_rep, b-
 bool fp64(const qcd_batch* b) { return b->common.precision == QCD_PREC_FP64; }
 
 int batch_pass(qcd_batch* b, int kind, int renorm) {
-  BatchArgs a{b->common.epsilon, b->common.upd, b->err, b->accept, renorm};
+  BatchArgs a{b->common.epsilon, b->common.upd, b->err, b->accept, renorm, b->draw_dev, 0};
   for (int k = 0; k < 6; k++) {
+    a.phase_off = (unsigned int)k;
     if (fp64(b))
       batch_phase_fn<true>(k, kind)<<<b->ctas, kBlock, 0, b->stream>>>(view(b), a);
     else
       batch_phase_fn<false>(k, kind)<<<b->ctas, kBlock, 0, b->stream>>>(view(b), a);
+    BCUDA(b, cudaGetLastError());
+  }
+  if (kind != KIND_OR) {
+    advance_counter<<<1, 1, 0, b->stream>>>(b->draw_dev, 6ull);
     BCUDA(b, cudaGetLastError());
   }
   return QCD_OK;
@@ -343,6 +354,7 @@ void release(qcd_batch* b) {
   cudaFree(b->rng);
   cudaFree(b->accept);
   cudaFree(b->err);
+  cudaFree(b->draw_dev);
   cudaFree(b->partials);
   cudaFree(b->rep_count);
   cudaFree(b->all_count);
@@ -434,6 +446,8 @@ int qcd_batch_create(const qcd_replica* r, int n, const qcd_params* common, qcd_
     if (rc == QCD_OK) step(cudaMemsetAsync(b->accept, 0, site_off * sizeof(int), b->stream), "memset");
   }
   if (rc == QCD_OK) step(cudaMalloc(&b->err, sizeof(int)), "cudaMalloc(err)");
+  if (rc == QCD_OK) step(cudaMalloc(&b->draw_dev, sizeof(unsigned long long)), "cudaMalloc(draw counter)");
+  if (rc == QCD_OK) step(cudaMemsetAsync(b->draw_dev, 0, sizeof(unsigned long long), b->stream), "memset");
   if (rc == QCD_OK) step(cudaMalloc(&b->partials, (size_t)cta * sizeof(double2)), "cudaMalloc(partials)");
   if (rc == QCD_OK) step(cudaMalloc(&b->rep_count, n * sizeof(unsigned int)), "cudaMalloc(counters)");
   if (rc == QCD_OK) step(cudaMalloc(&b->all_count, sizeof(unsigned int)), "cudaMalloc(counters)");
@@ -480,6 +494,9 @@ int qcd_batch_init(qcd_batch* b) {
     batch_setup<false><<<b->ctas, kBlock, 0, b->stream>>>(view(b));
   BCUDA(b, cudaGetLastError());
   BCUDA(b, cudaMemsetAsync(b->cursor, 0, sizeof(int), b->stream));
+  // a fresh start: the streams are re-seeded above, the counter of the FP32
+  // draws starts again at 0 (as for a newly created lattice)
+  BCUDA(b, cudaMemsetAsync(b->draw_dev, 0, sizeof(unsigned long long), b->stream));
   b->sweeps_done = 0;
   return QCD_OK;
 }

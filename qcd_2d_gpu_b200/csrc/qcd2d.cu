@@ -45,6 +45,11 @@ struct qcd_lattice {
   // conversion staging for host configs
   double* aos_stage = nullptr;
   long long sweeps_done = 0;
+  // drawing phases run so far (6 per heat-bath or Metropolis pass), on the
+  // device: the counter of the FP32 Philox draws, part of the generator
+  // checkpoint
+  unsigned long long* draw_dev = nullptr;
+  unsigned long long draw_key = 0;  // key of the FP32 draws: the seed, or the one a checkpoint restored
   // wavefront scheduler
   int sched = QCD_SCHED_AUTO;
   unsigned int* wave_done = nullptr;   // Lt arrival counters
@@ -151,9 +156,10 @@ Phase32Fn phase_fn32(int k, int bc, int kind) {
 // one pass over the six phases with one update kind; with `renorm` (FP32
 // only) every link is re-projected as it is stored
 int pass(qcd_lattice* h, int kind, int renorm = 0) {
-  PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, renorm};
+  PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, renorm, h->draw_key, h->draw_dev, 0, 0};
   const dim3 grid(nblocks(h->g.slice), (unsigned int)h->g.lt);
   for (int k = 0; k < 6; k++) {
+    a.phase_off = (unsigned int)k;
     if (h->p.precision == QCD_PREC_FP64)
       phase_fn64(k, h->p.boundary, kind)<<<grid, kBlock, 0, h->stream>>>(links64(h), rngs(h), h->g, a);
     else
@@ -161,6 +167,10 @@ int pass(qcd_lattice* h, int kind, int renorm = 0) {
     LAUNCH_CHECK(h);
   }
   if (kind != KIND_METRO) h->unit_passes++;
+  if (kind != KIND_OR) {
+    advance_counter<<<1, 1, 0, h->stream>>>(h->draw_dev, 6ull);
+    LAUNCH_CHECK(h);
+  }
   return QCD_OK;
 }
 
@@ -364,6 +374,10 @@ int launch_wave(qcd_lattice* h, const PassSpec* ps, int np, int stall_test = 0,
     S.kind[n] = (signed char)ps[n / 6].kind;
     S.renorm[n] = (signed char)ps[n / 6].renorm;
   }
+  for (int n = 0, d = 0; n < S.P; n++) {  // drawing phases numbered in program order
+    S.draw[n] = (unsigned char)d;
+    if (S.kind[n] != KIND_OR) d++;
+  }
   rc = plan_wave(mu, par, S.P, S.need, S.seam, S.start);
   if (rc) return fail(h, rc, "wavefront plan failed");
   S.lt = h->g.lt;
@@ -383,7 +397,7 @@ int launch_wave(qcd_lattice* h, const PassSpec* ps, int np, int stall_test = 0,
   CUDA_OR_FAIL(h, cudaMemsetAsync(h->wave_done, 0, (size_t)h->g.lt * sizeof(unsigned int), h->stream));
   CUDA_OR_FAIL(h, cudaMemsetAsync(h->wave_queue, 0, sizeof(unsigned int), h->stream));
   CUDA_OR_FAIL(h, cudaMemsetAsync(h->wave_abort, 0, sizeof(int), h->stream));
-  PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, 0};
+  PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, 0, h->draw_key, h->draw_dev, 0, 0};
   const int sk = h->p.algo == QCD_ALGO_HEATBATH ? KIND_HB : KIND_METRO;
   const int bc = h->p.boundary;
   const unsigned int grid = (unsigned int)h->wave_grid;
@@ -412,8 +426,15 @@ int launch_wave(qcd_lattice* h, const PassSpec* ps, int np, int stall_test = 0,
     }
   }
   LAUNCH_CHECK(h);
-  for (int i = 0; i < np; i++)
+  unsigned long long drawn = 0;
+  for (int i = 0; i < np; i++) {
     if (ps[i].kind != KIND_METRO) h->unit_passes++;
+    if (ps[i].kind != KIND_OR) drawn += 6;
+  }
+  if (drawn) {
+    advance_counter<<<1, 1, 0, h->stream>>>(h->draw_dev, drawn);
+    LAUNCH_CHECK(h);
+  }
   return QCD_OK;
 }
 
@@ -502,6 +523,7 @@ void release(qcd_lattice* h) {
   cudaFree(h->counter);
   cudaFree(h->result);
   cudaFree(h->err);
+  cudaFree(h->draw_dev);
   cudaFree(h->series);
   cudaFree(h->aos_stage);
   cudaFree(h->wave_done);
@@ -568,6 +590,7 @@ int qcd_create(const qcd_params* p, qcd_lattice** out) {
   h->p = *p;
   h->V = V;
   h->g = make_geo(p->lt, p->lx, p->ly);
+  h->draw_key = p->seed;
   const size_t vh = (size_t)h->g.vh;
   int rc = QCD_OK;
   auto step = [&](cudaError_t e, const char* what) {
@@ -597,6 +620,8 @@ int qcd_create(const qcd_params* p, qcd_lattice** out) {
   if (rc == QCD_OK) step(cudaMalloc(&h->counter, sizeof(unsigned int)), "cudaMalloc(counter)");
   if (rc == QCD_OK) step(cudaMalloc(&h->result, 2 * sizeof(double)), "cudaMalloc(result)");
   if (rc == QCD_OK) step(cudaMalloc(&h->err, sizeof(int)), "cudaMalloc(err)");
+  if (rc == QCD_OK) step(cudaMalloc(&h->draw_dev, sizeof(unsigned long long)), "cudaMalloc(draw counter)");
+  if (rc == QCD_OK) step(cudaMemsetAsync(h->draw_dev, 0, sizeof(unsigned long long), h->stream), "memset");
   if (rc == QCD_OK) step(cudaMallocHost(&h->result_host, 4 * sizeof(double)), "cudaMallocHost");
   if (rc == QCD_OK) step(cudaMemsetAsync(h->counter, 0, sizeof(unsigned int), h->stream), "memset");
   if (rc == QCD_OK) step(cudaMemsetAsync(h->err, 0, sizeof(int), h->stream), "memset");
@@ -845,6 +870,9 @@ int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
   if (acc_save)
     CUDA_OR_FAIL(h, cudaMemcpyAsync(acc_save, h->accept, (size_t)h->V * sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
   const long long passes_save = h->unit_passes, sweeps_save = h->sweeps_done;
+  unsigned long long draws_save = 0;
+  CUDA_OR_FAIL(h, cudaMemcpyAsync(&draws_save, h->draw_dev, sizeof(draws_save), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_OR_FAIL(h, cudaStreamSynchronize(h->stream));
   const int sched_save = h->sched, chunk_save = h->wave_chunk, chain_save = h->wave_chain, fronts_save = h->wave_fronts;
   cudaEvent_t e0, e1;
   CUDA_OR_FAIL(h, cudaEventCreate(&e0));
@@ -874,6 +902,8 @@ int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
   cudaFree(links2_save);
   cudaFree(rng_save);
   cudaFree(acc_save);
+  cudaMemcpyAsync(h->draw_dev, &draws_save, sizeof(draws_save), cudaMemcpyHostToDevice, h->stream);
+  cudaStreamSynchronize(h->stream);
   h->unit_passes = passes_save;
   h->sweeps_done = sweeps_save;
   h->sched = sched_save;
@@ -1008,23 +1038,41 @@ int qcd_check_unitarity(qcd_lattice* h, double tol, double* mean_det) {
   return QCD_OK;
 }
 
-// The six u32 words of each of the V/2 MRG32k3a streams, plane by plane
-// (word j of stream id at [j * V/2 + id]).  The reference keeps no generator
-// state across runs (a restart re-seeds, kernel.cu:79); saving it next to the
-// configuration makes a resumed run continue the exact same chain.
+// The generator checkpoint: the six u32 words of each of the V/2 MRG32k3a
+// streams, plane by plane (word j of stream id at [j * V/2 + id]), then the
+// drawing-phase counter and the key of the FP32 Philox draws (low word
+// first).  The reference keeps no generator state across runs (a restart
+// re-seeds, kernel.cu:79); saving it next to the configuration makes a
+// resumed run continue the exact same chain.
+long long qcd_rng_words(const qcd_lattice* h) { return h ? 6 * (long long)h->g.vh + 4 : 0; }
+
 int qcd_store_rng(qcd_lattice* h, uint32_t* host_out) {
   if (!h || !host_out) return QCD_ERR_INVALID;
-  CUDA_OR_FAIL(h, cudaMemcpyAsync(host_out, h->rng, 6 * (size_t)h->g.vh * sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                  h->stream));
-  return check_device_error(h);
+  const size_t n = 6 * (size_t)h->g.vh;
+  CUDA_OR_FAIL(h, cudaMemcpyAsync(host_out, h->rng, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  unsigned long long* c = reinterpret_cast<unsigned long long*>(&h->result_host[3]);
+  CUDA_OR_FAIL(h, cudaMemcpyAsync(c, h->draw_dev, sizeof(*c), cudaMemcpyDeviceToHost, h->stream));
+  int rc = check_device_error(h);  // synchronises the stream
+  host_out[n] = (uint32_t)*c;
+  host_out[n + 1] = (uint32_t)(*c >> 32);
+  host_out[n + 2] = (uint32_t)h->draw_key;
+  host_out[n + 3] = (uint32_t)(h->draw_key >> 32);
+  return rc;
 }
 
 int qcd_load_rng(qcd_lattice* h, const uint32_t* host_in) {
   if (!h || !host_in) return QCD_ERR_INVALID;
-  CUDA_OR_FAIL(h, cudaMemcpyAsync(h->rng, host_in, 6 * (size_t)h->g.vh * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                                  h->stream));
+  const size_t n = 6 * (size_t)h->g.vh;
+  const unsigned long long c = (unsigned long long)host_in[n] | ((unsigned long long)host_in[n + 1] << 32);
+  CUDA_OR_FAIL(h, cudaMemcpyAsync(h->rng, host_in, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+  CUDA_OR_FAIL(h, cudaMemcpyAsync(h->draw_dev, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream));
   CUDA_OR_FAIL(h, cudaStreamSynchronize(h->stream));
+  h->draw_key = (unsigned long long)host_in[n + 2] | ((unsigned long long)host_in[n + 3] << 32);
   return QCD_OK;
+}
+
+void qcd_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  Philox4x32::block(ctr, key, out);
 }
 
 long long qcd_volume(const qcd_lattice* h) { return h ? h->V : 0; }

@@ -53,4 +53,84 @@ struct RngStoreT {
 };
 typedef RngStoreT<false> RngStore;
 
+// ------------------------------------------------ counter-based stream ----
+// Philox4x32-10 (J. K. Salmon, M. A. Moraes, R. O. Dror, D. E. Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC'11): a 4 x 32-bit counter
+// and a 2 x 32-bit key go through ten rounds of two 32 x 32 -> 64-bit
+// multiplies with the round keys bumped by the Weyl increments between
+// rounds.  It keeps no state in memory: the FP32 sweep draws from the counter
+// (site, block, phase counter) under the key (seed), which removes the 2 x 24 B
+// of generator-state traffic per site and phase that a stored generator costs.
+struct Philox4x32 {
+  static constexpr uint32_t kM0 = 0xD2511F53u, kM1 = 0xCD9E8D57u;  // round multipliers
+  static constexpr uint32_t kW0 = 0x9E3779B9u, kW1 = 0xBB67AE85u;  // key increments
+  __host__ __device__ __forceinline__ static void block(const uint32_t ctr[4], const uint32_t key[2],
+                                                        uint32_t out[4]) {
+    uint32_t x0 = ctr[0], x1 = ctr[1], x2 = ctr[2], x3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+      if (r) {
+        k0 += kW0;
+        k1 += kW1;
+      }
+      const uint64_t p0 = (uint64_t)kM0 * x0, p1 = (uint64_t)kM1 * x2;
+      const uint32_t y0 = (uint32_t)(p1 >> 32) ^ x1 ^ k0;
+      const uint32_t y2 = (uint32_t)(p0 >> 32) ^ x3 ^ k1;
+      x1 = (uint32_t)p1;
+      x3 = (uint32_t)p0;
+      x0 = y0;
+      x2 = y2;
+    }
+    out[0] = x0;
+    out[1] = x1;
+    out[2] = x2;
+    out[3] = x3;
+  }
+};
+
+// The draws of one link update: counter (site, block, phase lo, phase hi),
+// block = 0, 1, ... as the update consumes 32-bit words in order.  `phase`
+// numbers the drawing phases of the lattice (6 per heat-bath or Metropolis
+// pass), so no two updates share a counter.
+struct PhiloxStream {
+  uint32_t key[2], ctr[4];
+  uint32_t b0, b1, b2, b3;
+  int left;
+  __device__ __forceinline__ PhiloxStream(unsigned long long seed, uint32_t site, unsigned long long phase) {
+    key[0] = (uint32_t)seed;
+    key[1] = (uint32_t)(seed >> 32);
+    ctr[0] = site;
+    ctr[1] = 0;
+    ctr[2] = (uint32_t)phase;
+    ctr[3] = (uint32_t)(phase >> 32);
+    left = 0;
+  }
+  __device__ __forceinline__ uint32_t next() {
+    if (left == 0) {
+      uint32_t o[4];
+      Philox4x32::block(ctr, key, o);
+      ctr[1]++;
+      b0 = o[0];
+      b1 = o[1];
+      b2 = o[2];
+      b3 = o[3];
+      left = 4;
+    }
+    const uint32_t v = b0;  // rotate through registers (no indexed local array)
+    b0 = b1;
+    b1 = b2;
+    b2 = b3;
+    left--;
+    return v;
+  }
+  // (k + 1) / 2^24 for the top 24 bits k: exact floats in (0, 1]
+  __device__ __forceinline__ float uniform() { return (float)((next() >> 8) + 1u) * 5.9604644775390625e-8f; }
+  // (k + 1) / 2^53 from 53 bits of two words: exact doubles in (0, 1]
+  __device__ __forceinline__ double uniform_double() {
+    const uint64_t hi = next(), lo = next();
+    return (double)(((hi << 21) | (lo >> 11)) + 1ull) * 1.1102230246251565e-16;
+  }
+};
+
 }  // namespace qcd

@@ -20,7 +20,27 @@ struct PhaseArgs {
   int* err;     // device error word
   int* accept;  // V ints, reference site order; only for Metropolis
   int renorm;   // FP32: re-project each updated link (in double) before it is stored
+  // FP32 draws (counter-based): the key, the device word holding the number
+  // of drawing phases run before this launch (advanced on the device, so a
+  // captured graph draws fresh numbers on every replay), this phase's offset
+  // from it, and the offset added to the site index (a replica's stream
+  // offset in a batch)
+  unsigned long long seed;
+  const unsigned long long* phase_ptr;
+  unsigned int phase_off;
+  unsigned int site_off;
 };
+
+// The drawing-phase counter of the FP32 draws lives on the device and is
+// advanced by this one-thread launch after every heat-bath or Metropolis pass
+// (inside a captured graph too).  Internal linkage: each translation unit
+// that includes this header has its own copy.
+static __global__ void advance_counter(unsigned long long* c, unsigned long long n) { *c += n; }
+
+// the drawing-phase number of this launch
+__device__ __forceinline__ unsigned long long draw_phase(const PhaseArgs& a) {
+  return __ldg(a.phase_ptr) + a.phase_off;
+}
 
 // ------------------------------------------------------- one link update --
 // Update U_MU at site n of sublattice PAR: the body of the six launches of
@@ -61,6 +81,9 @@ __device__ __forceinline__ void site64(const Links64T<CG>& L, const RngStoreT<CG
   }
 }
 
+// FP32: the same updates with FP32 links and FP64 fix-ups; the heat-bath and
+// Metropolis draw from the counter-based Philox stream of (site, phase), so
+// no generator state is read or written.
 template <int MU, int PAR, int BC, int KIND, bool CG>
 __device__ __forceinline__ void site32(const Links32T<CG>& L, const RngStoreT<CG>& R, const Geo& g,
                                        const PhaseArgs& a, const Nbr& n, int renorm) {
@@ -69,16 +92,12 @@ __device__ __forceinline__ void site32(const Links32T<CG>& L, const RngStoreT<CG
   Quat<float> A = staple_sum<MU, BC, Links32T<CG>, float>(L, g, n, PAR);
   Quat<float> U;
   if (KIND == KIND_HB) {
-    curandStateMRG32k3a_t st;
-    R.load(id, &st);
-    U = heatbath_fast(A, a.beta, &st, a.err);
-    R.store(id, &st);
+    PhiloxStream st(a.seed, a.site_off + (unsigned int)id, draw_phase(a));
+    U = heatbath_fast(A, a.beta, st, a.err);
   } else if (KIND == KIND_METRO) {
-    curandStateMRG32k3a_t st;
-    R.load(id, &st);
+    PhiloxStream st(a.seed, a.site_off + (unsigned int)id, draw_phase(a));
     U = L.ld_own(MU, PAR, id);
-    int acc = metropolis_fast(U, A, a.beta, a.eps, a.upd, &st);
-    R.store(id, &st);
+    int acc = metropolis_fast(U, A, a.beta, a.eps, a.upd, st);
     add_accept<CG>(a.accept + PAR * g.vh + id, acc);
   } else {
     U = overrelax_fast(A, L.ld_own(MU, PAR, id));

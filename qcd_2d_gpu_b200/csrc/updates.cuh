@@ -148,13 +148,15 @@ __device__ __forceinline__ Quat<double> overrelax_ref(Quat<double> A, const Quat
 }
 
 // ------------------------------------------- FP32 links + FP64 fix-ups ----
+// The FP32 updates draw from a generator G with uniform() (float in (0, 1])
+// and uniform_double() (double in (0, 1]): the counter-based PhiloxStream.
 
 // Kennedy-Pendleton in FP32.  The parts that lose accuracy in single precision
 // are done in double: the accept test (1 - lf is within an ulp of 1 for large
 // beta*|A|) and the length of the spatial part, n = 2 sqrt(lf (1 - lf)),
 // which replaces sqrt(1 - X0^2) and its cancellation as X0 -> 1.
-__device__ __forceinline__ Quat<float> heatbath_fast(Quat<float> A, float beta,
-                                                     curandStateMRG32k3a_t* st, int* err) {
+template <class G>
+__device__ __forceinline__ Quat<float> heatbath_fast(Quat<float> A, float beta, G& st, int* err) {
   float det = q_det(A);
   float rinv = rsqrtf(det);
   float a = det * rinv;
@@ -163,12 +165,12 @@ __device__ __forceinline__ Quat<float> heatbath_fast(Quat<float> A, float beta,
   float lf;
   float aux;
   for (int tries = 1;; tries++) {
-    float r0 = curand_uniform(st), r1 = curand_uniform(st), r2 = curand_uniform(st);
+    float r0 = st.uniform(), r1 = st.uniform(), r2 = st.uniform();
     // hardware approximations (absolute error ~2^-21): cos(2 pi r1) evaluated
     // as -cos(2 pi (r1 - 1/2)) keeps the argument in [-pi, pi]
     float c = -__cosf(6.2831853f * (r1 - 0.5f));
     lf = -(__logf(r0) + c * c * __logf(r2)) * inv;
-    aux = 1.f - curand_uniform(st);
+    aux = 1.f - st.uniform();
     if (!((double)aux * aux > 1.0 - (double)lf)) break;
     if (tries >= QCD_HB_MAX_TRIES) {
       atomicOr(err, DEVERR_HB_LOOP);
@@ -178,8 +180,8 @@ __device__ __forceinline__ Quat<float> heatbath_fast(Quat<float> A, float beta,
   double lfd = lf;
   float x0 = (float)(1.0 - 2.0 * lfd);
   float nrm = (float)(2.0 * sqrt(lfd * (1.0 - lfd)));
-  float ct = 2.f * curand_uniform(st) - 1.f, sp, cp;
-  __sincosf(6.2831853f * (curand_uniform(st) - 0.5f), &sp, &cp);  // angle + pi
+  float ct = 2.f * st.uniform() - 1.f, sp, cp;
+  __sincosf(6.2831853f * (st.uniform() - 0.5f), &sp, &cp);  // angle + pi
   float stt = sqrtf(fmaxf(0.f, 1.f - ct * ct));
   Quat<float> X{x0, nrm * ct, -nrm * stt * cp, -nrm * stt * sp};
   return q_mul_bd(X, A);
@@ -193,20 +195,21 @@ __device__ __forceinline__ Quat<float> overrelax_fast(Quat<float> A, const Quat<
 
 // Metropolis with FP32 links: proposal and action change in float, the
 // accept decision with the same single-then-double test as the reference.
+template <class G>
 __device__ __forceinline__ int metropolis_fast(Quat<float>& U, const Quat<float>& A, float beta,
-                                               float eps, int upd, curandStateMRG32k3a_t* st) {
+                                               float eps, int upd, G& st) {
   int acc = 0;
   const float r0 = sqrtf(1.f - eps * eps);
   for (int h = 0; h < upd; h++) {
-    float r1 = curand_uniform(st) - 0.5f;
-    float r2 = curand_uniform(st) - 0.5f;
-    float r3 = curand_uniform(st) - 0.5f;
+    float r1 = st.uniform() - 0.5f;
+    float r2 = st.uniform() - 0.5f;
+    float r3 = st.uniform() - 0.5f;
     float sc = eps * rsqrtf(r1 * r1 + r2 * r2 + r3 * r3);
     Quat<float> r{r0, sc * r1, sc * r2, sc * r3};
     Quat<float> Un = q_mul(r, U);
     Quat<float> dU{Un.w - U.w, Un.x - U.x, Un.y - U.y, Un.z - U.z};
     double s = -(double)beta * (double)q_retr_mul(dU, A);
-    bool ok = s < 0 ? true : metropolis_accept(s, curand_uniform_double(st));
+    bool ok = s < 0 ? true : metropolis_accept(s, st.uniform_double());
     if (ok) {
       U = Un;
       acc++;

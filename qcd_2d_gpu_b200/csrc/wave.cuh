@@ -40,6 +40,7 @@ struct WaveSched {
   signed char mu[kMaxWavePhases], par[kMaxWavePhases], kind[kMaxWavePhases], renorm[kMaxWavePhases];
   short need[3][kMaxWavePhases];  // latest earlier phase waited for at t-1, t, t+1 (-1: none)
   int seam[kMaxWavePhases], start[kMaxWavePhases];
+  unsigned char draw[kMaxWavePhases];  // drawing-phase offset from the launch's counter (FP32 draws)
 };
 
 struct WaveCtl {
@@ -179,7 +180,9 @@ __global__ void __launch_bounds__(kBlock, 5) wave(LinksT L, RngStoreT<true> R, G
     const int type = S.mu[n] * 2 + S.par[n], kind = S.kind[n], rn = S.renorm[n];
     const int s0 = sh_chunk * S.chunk_sites;
     const int s1 = min(s0 + S.chunk_sites, g.slice);
-    for (int s = s0 + (int)threadIdx.x; s < s1; s += kBlock) wave_site<BC, SK>(L, R, g, a, type, kind, rn, s, t);
+    PhaseArgs an = a;
+    an.phase_off = S.draw[n];
+    for (int s = s0 + (int)threadIdx.x; s < s1; s += kBlock) wave_site<BC, SK>(L, R, g, an, type, kind, rn, s, t);
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();

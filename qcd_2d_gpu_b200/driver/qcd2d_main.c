@@ -143,7 +143,7 @@ static int parse(int argc, char** argv, knobs* k) {
   return 0;
 }
 
-/* Config_<...>_rng.bin: the 6 x V/2 u32 generator words (qcd_store_rng) */
+/* Config_<...>_rng.bin: the qcd_rng_words u32 generator words (qcd_store_rng) */
 static void rng_path(char* out, size_t cap, const char* dir, const refio_lattice* l, const char* bound,
                      const char* n) {
   snprintf(out, cap, "%s%sConfig_%d_%d_%d_B_%.2lf_%s_%s_rng.bin", dir, dir[0] ? "/" : "", l->t, l->x, l->y,
@@ -222,7 +222,7 @@ int main(int argc, char** argv) {
     if (k.rng_state) {  // resume the generator chain saved with the configuration
       char rp[1024];
       rng_path(rp, sizeof(rp), k.outdir, &l, bound, k.nconfr);
-      const size_t nw = 6 * (size_t)(l.V / 2);
+      const size_t nw = (size_t)qcd_rng_words(h);
       unsigned int* w = (unsigned int*)malloc(nw * sizeof(unsigned int));
       FILE* f = fopen(rp, "rb");
       if (!w || !f || fread(w, sizeof(unsigned int), nw, f) != nw) {
@@ -263,7 +263,7 @@ int main(int argc, char** argv) {
       if (k.rng_state) {
         char rp[1024];
         rng_path(rp, sizeof(rp), k.outdir, &l, bound, k.nconfs);
-        const size_t nw = 6 * (size_t)(l.V / 2);
+        const size_t nw = (size_t)qcd_rng_words(h);
         unsigned int* w = (unsigned int*)malloc(nw * sizeof(unsigned int));
         if (!w) exit(1);
         CHECK(qcd_store_rng(h, w));

@@ -61,3 +61,62 @@ def test_fp32_overrelaxation_conserves_action_to_float_accuracy():
     p0 = L.measure()[1]
     L.overrelax(10)
     assert abs(L.measure()[1] - p0) < 1e-5
+
+
+# ---- the counter-based draws of the FP32 sweep ------------------------------
+@pytest.mark.parametrize("algo,bc,n_or", [("hb", 2, 3), ("metro", 1, 1)])
+def test_fp32_generator_checkpoint_resumes_the_chain_exactly(algo, bc, n_or):
+    kw = dict(algo=algo, boundary=bc, precision="fp32", n_or=n_or, renorm_every=1, epsilon=0.3, upd=2)
+    a = q.Lattice(8, 8, 12, 6.5, seed=21, **kw)
+    a.init_hot()
+    a.sweep(10)
+    b = q.Lattice(8, 8, 12, 6.5, seed=21, **kw)
+    b.init_hot()
+    b.sweep(5)
+    cfg, rng = b.store_config(), b.store_rng()
+    c = q.Lattice(8, 8, 12, 6.5, seed=999, **kw)  # the key comes from the checkpoint
+    c.load_config(cfg)
+    c.load_rng(rng)
+    c.sweep(5)
+    assert np.array_equal(c.store_config(), a.store_config())
+    # accept counts are not part of the checkpoint: c counted only its own 5 sweeps
+    assert np.array_equal(c.accept_counts(), a.accept_counts() - b.accept_counts())
+    for L in (a, b, c):
+        L.close()
+
+
+def test_fp32_sweeps_replayed_from_a_captured_graph_draw_fresh_numbers():
+    # the drawing-phase counter lives on the device: each replay of a captured
+    # sweep advances it, so two replays equal two sweeps run directly
+    import torch
+
+    kw = dict(boundary=2, precision="fp32", n_or=1, renorm_every=1, seed=8)
+    direct = q.Lattice(8, 8, 16, 7.0, **kw)
+    direct.init_hot()
+    direct.sweep(3)
+    s = torch.cuda.Stream()
+    G = q.Lattice(8, 8, 16, 7.0, **kw)
+    G.set_stream(s.cuda_stream)
+    G.init_hot()
+    G.sweep(1)  # the first sweep runs directly
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        G.sweep(1)  # captured, not run
+    g.replay()
+    g.replay()
+    torch.cuda.synchronize()
+    assert np.array_equal(G.store_config(), direct.store_config())
+    for L in (direct, G):
+        L.close()
+
+
+def test_fp32_seeds_give_different_chains():
+    f = []
+    for seed in (1, 2):
+        L = q.Lattice(8, 8, 8, 6.0, precision="fp32", seed=seed)
+        L.init_cold()  # the same start: only the draws differ
+        L.sweep(2)
+        f.append(L.store_config())
+        L.close()
+    assert not np.array_equal(f[0], f[1])
