@@ -512,7 +512,7 @@ def main():
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f32+f64-fixups",
-            "data": "synthetic (hot start, seeded MRG32k3a)",
+            "data": "synthetic (hot start from seeded MRG32k3a streams; FP32 draws from Philox4x32-10)",
             "config": {"workload": f"{LT}x{LX}x{LY} PMC, hot start, sweep = 1 heat-bath + {N_OR} "
                                    f"over-relaxation, FP32 links + FP64 fix-ups, renormalise every sweep, "
                                    f"measure every {N_COR} sweeps",
