@@ -441,10 +441,10 @@ def main():
     hb_launch_ms = hb_pass_ms / n_launch
     L2h.close()
     # strict algorithmic bytes: each FP32 link read once and written once per
-    # pass (32 B per update), plus for the heat-bath 2 x 24 B of MRG32k3a state
-    # per 6 updates (40 B per update); a pass is 3V updates
+    # pass, 32 B per update (the FP32 heat-bath draws keep no generator state);
+    # a pass is 3V updates
     or_bytes = 32.0 * 3 * V / n_launch
-    hb_bytes = 40.0 * 3 * V / n_launch
+    hb_bytes = 32.0 * 3 * V / n_launch
     hbm, peak_kind = peaks()
     or_gbs = or_bytes / (or_launch_ms * 1e-3) / 1e9
     roofline = {"kernel": "phase32<mu, par, PMC, OR> (over-relaxation phase)", "bound": "hbm", "achieved": or_gbs,

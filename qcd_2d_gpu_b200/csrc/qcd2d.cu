@@ -439,11 +439,9 @@ int launch_wave(qcd_lattice* h, const PassSpec* ps, int np, int stall_test = 0,
 }
 
 bool use_wave(const qcd_lattice* h) {
-  if (h->sched == QCD_SCHED_WAVEFRONT) return true;
-  if (h->sched == QCD_SCHED_PHASES) return false;
-  // automatic: per-phase launches (measured faster on B200 at every size so
-  // far); the wavefront is selected explicitly
-  return false;
+  // automatic never picks the wavefront: per-phase launches measured faster
+  // on B200 at every size tried; the wavefront is selected explicitly
+  return h->sched == QCD_SCHED_WAVEFRONT;
 }
 
 int run_passes(qcd_lattice* h, const PassSpec* ps, int np);
