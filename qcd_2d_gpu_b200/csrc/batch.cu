@@ -36,6 +36,7 @@ struct Replica {
   long long rng_off;   // u32 words
   long long site_off;  // accept counters
   int cta_begin;       // first CTA of this replica in a batched launch
+  int mcta_begin;      // first CTA of this replica in a batched measurement (measure_blocks per replica)
   unsigned long long seed;
   long long stream_off;
 };
@@ -43,6 +44,7 @@ struct Replica {
 struct BatchView {
   const Replica* rep;
   const int* cta_rep;  // replica of every CTA of a batched launch
+  const int* mcta_rep; // replica of every CTA of a batched measurement
   int n;
   float4* q32;
   double2* lo;
@@ -146,42 +148,36 @@ __global__ void __launch_bounds__(kBlock) batch_normalize(BatchView B) {
 
 // energy / plaquette of every replica (en_av semantics, observables.h:99-141)
 // into series[r * cap + *cursor]; per-replica fixed-order sums as in measure<>
+// Energy and plaquette of every replica into series[r * cap + k], k the
+// device cursor.  Each replica's CTAs cover it as a single-lattice
+// measurement does (measure_blocks CTAs striding over its sites) and its last
+// CTA adds their partials in the same order, so every replica's numbers are
+// those of the same lattice measured alone, bit for bit.
 template <bool FP64>
 __global__ void __launch_bounds__(kBlock) batch_measure(BatchView B, double2* partials, unsigned int* rep_count,
                                                         unsigned int* all_count, int* cursor, double2* series,
                                                         int cap) {
-  const int r = replica_of(B, blockIdx.x);
+  const int r = __ldg(B.mcta_rep + blockIdx.x);
   const Replica& R = B.rep[r];
-  const int id = (blockIdx.x - R.cta_begin) * kBlock + threadIdx.x;
+  const int nblk = (int)measure_blocks(R.g.vh);
   const int k = *(volatile int*)cursor;  // advanced only by the last CTA below
   double e = 0, pl = 0;
-  if (id < R.g.vh) {
-    for (int p = 0; p < 2; p++) {
-      const Nbr n = make_nbr(R.g, id, p);
-      double a, b, c;
-      if (FP64) {
-        Links64 L{B.lo + R.link_off, B.hi + R.link_off, R.g.vh};
-        a = plaq(L, DIR_Y, DIR_X, p, id, n.yp, n.xp);
-        b = plaq(L, DIR_Y, DIR_T, p, id, n.yp, n.tp);
-        c = plaq(L, DIR_X, DIR_T, p, id, n.xp, n.tp);
-      } else {
-        Links32 L{B.q32 + R.link_off, R.g.vh};
-        a = plaq(L, DIR_Y, DIR_X, p, id, n.yp, n.xp);
-        b = plaq(L, DIR_Y, DIR_T, p, id, n.yp, n.tp);
-        c = plaq(L, DIR_X, DIR_T, p, id, n.xp, n.tp);
-      }
-      if (R.bc == BC_PMC && at_ytop(R.g, n)) {
-        a = 0;
-        b = 0;
-      }
-      e += -c;
-      pl += (3 - a - b - c) / 3;
-    }
+  if (FP64) {
+    Links64 L{B.lo + R.link_off, B.hi + R.link_off, R.g.vh};
+    if (R.bc == BC_PMC)
+      measure_sites<Links64, true>(L, R.g, blockIdx.x - R.mcta_begin, nblk, e, pl);
+    else
+      measure_sites<Links64, false>(L, R.g, blockIdx.x - R.mcta_begin, nblk, e, pl);
+  } else {
+    Links32 L{B.q32 + R.link_off, R.g.vh};
+    if (R.bc == BC_PMC)
+      measure_sites<Links32, true>(L, R.g, blockIdx.x - R.mcta_begin, nblk, e, pl);
+    else
+      measure_sites<Links32, false>(L, R.g, blockIdx.x - R.mcta_begin, nblk, e, pl);
   }
   double se, sp;
-  block_sum2(e, pl, &se, &sp);
+  block_sum2(e, pl * (1.0 / 3.0), &se, &sp);
   __shared__ bool last_rep, last_all;
-  const int nblk = (R.g.vh + kBlock - 1) / kBlock;
   if (threadIdx.x == 0) {
     partials[blockIdx.x] = make_double2(se, sp);
     __threadfence();
@@ -192,7 +188,7 @@ __global__ void __launch_bounds__(kBlock) batch_measure(BatchView B, double2* pa
     __threadfence();
     double a = 0, b = 0;
     for (int i = threadIdx.x; i < nblk; i += kBlock) {
-      double2 v = __ldcg(partials + R.cta_begin + i);
+      double2 v = __ldcg(partials + R.mcta_begin + i);
       a += v.x;
       b += v.y;
     }
@@ -248,6 +244,8 @@ struct qcd_batch {
   cudaStream_t own = nullptr, stream = nullptr;
   Replica* rep_dev = nullptr;
   int* cta_rep = nullptr;
+  int* mcta_rep = nullptr;
+  int mctas = 0;
   float4* q32 = nullptr;
   double2* lo = nullptr;
   double2* hi = nullptr;
@@ -290,7 +288,9 @@ int bfail(qcd_batch* b, int code, const char* fmt, ...) {
     }                                                                                               \
   } while (0)
 
-BatchView view(const qcd_batch* b) { return BatchView{b->rep_dev, b->cta_rep, b->n, b->q32, b->lo, b->hi, b->rng}; }
+BatchView view(const qcd_batch* b) {
+  return BatchView{b->rep_dev, b->cta_rep, b->mcta_rep, b->n, b->q32, b->lo, b->hi, b->rng};
+}
 
 bool fp64(const qcd_batch* b) { return b->common.precision == QCD_PREC_FP64; }
 
@@ -331,10 +331,10 @@ int batch_sweep(qcd_batch* b, bool renorm) {
 
 int batch_measure_launch(qcd_batch* b) {
   if (fp64(b))
-    batch_measure<true><<<b->ctas, kBlock, 0, b->stream>>>(view(b), b->partials, b->rep_count, b->all_count,
+    batch_measure<true><<<b->mctas, kBlock, 0, b->stream>>>(view(b), b->partials, b->rep_count, b->all_count,
                                                             b->cursor, b->series, b->cap);
   else
-    batch_measure<false><<<b->ctas, kBlock, 0, b->stream>>>(view(b), b->partials, b->rep_count, b->all_count,
+    batch_measure<false><<<b->mctas, kBlock, 0, b->stream>>>(view(b), b->partials, b->rep_count, b->all_count,
                                                              b->cursor, b->series, b->cap);
   BCUDA(b, cudaGetLastError());
   return QCD_OK;
@@ -348,6 +348,7 @@ void release(qcd_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   cudaFree(b->rep_dev);
   cudaFree(b->cta_rep);
+  cudaFree(b->mcta_rep);
   cudaFree(b->q32);
   cudaFree(b->lo);
   cudaFree(b->hi);
@@ -379,7 +380,7 @@ int qcd_batch_create(const qcd_replica* r, int n, const qcd_params* common, qcd_
   b->common = *common;
   b->n = n;
   long long link_off = 0, rng_off = 0, site_off = 0;
-  int cta = 0;
+  int cta = 0, mcta = 0;
   for (int i = 0; i < n; i++) {
     const qcd_replica& x = r[i];
     if (x.lt < 2 || x.lx < 2 || x.ly < 2 || (x.lt & 1) || (x.lx & 1) || (x.ly & 1) || !(x.beta > 0.f) ||
@@ -401,6 +402,7 @@ int qcd_batch_create(const qcd_replica* r, int n, const qcd_params* common, qcd_
     R.rng_off = rng_off;
     R.site_off = site_off;
     R.cta_begin = cta;
+    R.mcta_begin = mcta;
     R.seed = x.seed;
     R.stream_off = x.stream_offset;
     b->rep.push_back(R);
@@ -408,9 +410,11 @@ int qcd_batch_create(const qcd_replica* r, int n, const qcd_params* common, qcd_
     rng_off += 6 * (V / 2);
     site_off += V;
     cta += (int)((V / 2 + kBlock - 1) / kBlock);
+    mcta += (int)measure_blocks(V / 2);
   }
   b->sites = site_off;
   b->ctas = cta;
+  b->mctas = mcta;
   int rc = QCD_OK;
   auto step = [&](cudaError_t e, const char* what) {
     if (rc == QCD_OK && e != cudaSuccess) {
@@ -433,6 +437,15 @@ int qcd_batch_create(const qcd_replica* r, int n, const qcd_params* common, qcd_
     step(cudaMalloc(&b->cta_rep, (size_t)cta * sizeof(int)), "cudaMalloc(cta table)");
     if (rc == QCD_OK)
       step(cudaMemcpy(b->cta_rep, owner.data(), (size_t)cta * sizeof(int), cudaMemcpyHostToDevice), "cta table");
+    std::vector<int> mowner((size_t)mcta);
+    for (int i = 0; i < n; i++) {
+      const int end = i + 1 < n ? b->rep[i + 1].mcta_begin : mcta;
+      for (int c = b->rep[i].mcta_begin; c < end; c++) mowner[c] = i;
+    }
+    if (rc == QCD_OK) step(cudaMalloc(&b->mcta_rep, (size_t)mcta * sizeof(int)), "cudaMalloc(cta table)");
+    if (rc == QCD_OK)
+      step(cudaMemcpy(b->mcta_rep, mowner.data(), (size_t)mcta * sizeof(int), cudaMemcpyHostToDevice),
+           "cta table");
   }
   if (common->precision == QCD_PREC_FP64) {
     if (rc == QCD_OK) step(cudaMalloc(&b->lo, link_off * sizeof(double2)), "cudaMalloc(links)");
@@ -448,7 +461,8 @@ int qcd_batch_create(const qcd_replica* r, int n, const qcd_params* common, qcd_
   if (rc == QCD_OK) step(cudaMalloc(&b->err, sizeof(int)), "cudaMalloc(err)");
   if (rc == QCD_OK) step(cudaMalloc(&b->draw_dev, sizeof(unsigned long long)), "cudaMalloc(draw counter)");
   if (rc == QCD_OK) step(cudaMemsetAsync(b->draw_dev, 0, sizeof(unsigned long long), b->stream), "memset");
-  if (rc == QCD_OK) step(cudaMalloc(&b->partials, (size_t)cta * sizeof(double2)), "cudaMalloc(partials)");
+  if (rc == QCD_OK)
+    step(cudaMalloc(&b->partials, (size_t)(mcta > cta ? mcta : cta) * sizeof(double2)), "cudaMalloc(partials)");
   if (rc == QCD_OK) step(cudaMalloc(&b->rep_count, n * sizeof(unsigned int)), "cudaMalloc(counters)");
   if (rc == QCD_OK) step(cudaMalloc(&b->all_count, sizeof(unsigned int)), "cudaMalloc(counters)");
   if (rc == QCD_OK) step(cudaMalloc(&b->cursor, sizeof(int)), "cudaMalloc(cursor)");

@@ -159,24 +159,10 @@ __global__ void __launch_bounds__(kBlock) soa_to_aos32(Links32 L, double* __rest
 template <class L, int PMC>
 __global__ void __launch_bounds__(kBlock) measure(L links, Geo g, double2* partials,
                                                   unsigned int* counter, double* out) {
-  const int id = blockIdx.x * kBlock + threadIdx.x;
   double e = 0, pl = 0;
-  if (id < g.vh) {
-    for (int p = 0; p < 2; p++) {
-      const Nbr n = make_nbr(g, id, p);
-      double a = plaq(links, DIR_Y, DIR_X, p, id, n.yp, n.xp);
-      double b = plaq(links, DIR_Y, DIR_T, p, id, n.yp, n.tp);
-      double c = plaq(links, DIR_X, DIR_T, p, id, n.xp, n.tp);
-      if (PMC && at_ytop(g, n)) {
-        a = 0;
-        b = 0;
-      }
-      e += -c;
-      pl += (3 - a - b - c) / 3;
-    }
-  }
+  measure_sites<L, PMC != 0>(links, g, blockIdx.x, gridDim.x, e, pl);  // grid: measure_blocks(V/2)
   double se, sp;
-  block_sum2(e, pl, &se, &sp);
+  block_sum2(e, pl * (1.0 / 3.0), &se, &sp);
   if (threadIdx.x == 0) partials[blockIdx.x] = make_double2(se, sp);
   finish_sum2(partials, counter, 1.0 / (2.0 * (double)g.vh), out);
 }

@@ -8,6 +8,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <algorithm>
 #include <mutex>
 #include <new>
 #include <vector>
@@ -475,7 +476,7 @@ int reduce_result(qcd_lattice* h, double* a, double* b) {
 }
 
 int launch_measure(qcd_lattice* h, double* out_dev) {
-  const unsigned int nb = nblocks(h->g.vh);
+  const unsigned int nb = measure_blocks(h->g.vh);
   const bool pmc = h->p.boundary == QCD_BC_PMC;
   if (h->p.precision == QCD_PREC_FP64) {
     if (pmc)
@@ -613,7 +614,7 @@ int qcd_create(const qcd_params* p, qcd_lattice** out) {
     step(cudaMalloc(&h->accept, 2 * vh * sizeof(int)), "cudaMalloc(accept)");
     if (rc == QCD_OK) step(cudaMemsetAsync(h->accept, 0, 2 * vh * sizeof(int), h->stream), "memset");
   }
-  const size_t nb = nblocks(h->g.vh);
+  const size_t nb = nblocks(h->g.vh);  // one partial per CTA of the largest reduction launch
   if (rc == QCD_OK) step(cudaMalloc(&h->partials, nb * sizeof(double2)), "cudaMalloc(partials)");
   if (rc == QCD_OK) step(cudaMalloc(&h->counter, sizeof(unsigned int)), "cudaMalloc(counter)");
   if (rc == QCD_OK) step(cudaMalloc(&h->result, 2 * sizeof(double)), "cudaMalloc(result)");
@@ -1196,10 +1197,11 @@ extern "C" int qcd_measure_aos_noalloc(const double* phi_dev, int lt, int lx, in
   if (e == cudaSuccess) {
     Geo g = make_geo(lt, lx, ly);
     LinksAoS L{phi_dev, (int)vh};
+    const unsigned int grid = measure_blocks(vh);  // the same grid, so the same sums, as qcd_measure
     if (boundary == QCD_BC_PMC)
-      measure<LinksAoS, 1><<<(unsigned int)nb, kBlock, 0, s>>>(L, g, partials, counter, out_dev);
+      measure<LinksAoS, 1><<<grid, kBlock, 0, s>>>(L, g, partials, counter, out_dev);
     else
-      measure<LinksAoS, 0><<<(unsigned int)nb, kBlock, 0, s>>>(L, g, partials, counter, out_dev);
+      measure<LinksAoS, 0><<<grid, kBlock, 0, s>>>(L, g, partials, counter, out_dev);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) {

@@ -142,17 +142,18 @@ __device__ __forceinline__ void block_sum2(double v0, double v1, double* out0, d
 __device__ __forceinline__ void finish_sum2(double2* partials, unsigned int* counter, double scale,
                                             double* out) {
   __shared__ bool last;
+  const unsigned int ctas = gridDim.x;
   if (threadIdx.x == 0) {
     __threadfence();
     unsigned int prev = atomicAdd(counter, 1u);
-    last = (prev == gridDim.x - 1);
+    last = (prev == ctas - 1);
   }
   __syncthreads();
   if (!last) return;
   __threadfence();
   // fixed-order sum over partials: per-thread strided chunks, then the CTA tree
   double a = 0, b = 0;
-  for (unsigned int i = threadIdx.x; i < gridDim.x; i += kBlock) {
+  for (unsigned int i = threadIdx.x; i < ctas; i += kBlock) {
     double2 v = __ldcg(partials + i);  // L2: written by other CTAs
     a += v.x;
     b += v.y;
@@ -199,6 +200,40 @@ __device__ __forceinline__ double plaq(const L& links, int mu, int nu, int p, in
   Quat<double> B = q_mul_bd(A, ld64(links, mu, p ^ 1, id + onu));
   A = q_mul_bd(B, ld64(links, nu, p, id));
   return 1 - A.w;
+}
+
+// CTAs of a measurement: one per 256 sites up to a fixed cap, the threads
+// striding over the sites, so a large lattice makes a few thousand partial
+// sums (added by the last CTA).  The count depends on the lattice only, so
+// the summation order is the same on every device.
+constexpr long long kMeasureMaxBlocks = 4096;
+__host__ __device__ __forceinline__ unsigned int measure_blocks(long long vh) {
+  const long long nb = (vh + kBlock - 1) / kBlock;
+  return (unsigned int)(nb < kMeasureMaxBlocks ? nb : kMeasureMaxBlocks);
+}
+
+// Energy and plaquette sums of the sites id = c*256 + tid, + nb*256, ... of
+// CTA c of nb (both parities): -(1 - P_xt) and 3 - sum of the three 1 - P.
+// One division finds the site's t-slice; the neighbours come from the
+// slice position (multiply-high).
+template <class L, bool PMC>
+__device__ __forceinline__ void measure_sites(const L& links, const Geo& g, int c, int nb, double& e, double& pl) {
+  for (int id = c * kBlock + threadIdx.x; id < g.vh; id += nb * kBlock) {
+    const int t = id / g.slice;
+    const int s = id - t * g.slice;
+    for (int p = 0; p < 2; p++) {
+      const Nbr n = make_nbr_slice(g, s, t, p);
+      double a = plaq(links, DIR_Y, DIR_X, p, id, n.yp, n.xp);
+      double b = plaq(links, DIR_Y, DIR_T, p, id, n.yp, n.tp);
+      double cc = plaq(links, DIR_X, DIR_T, p, id, n.xp, n.tp);
+      if (PMC && at_ytop(g, n)) {
+        a = 0;
+        b = 0;
+      }
+      e += -cc;
+      pl += 3 - a - b - cc;  // the 1/3 of the plaquette average is applied once per thread
+    }
+  }
 }
 
 }  // namespace qcd
