@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(kBlock) batch_phase(BatchView B, BatchArgs a) 
   const Replica& R = B.rep[r];
   const int id = (blockIdx.x - R.cta_begin) * kBlock + threadIdx.x;
   if (id >= R.g.vh) return;
-  const Nbr n = make_nbr(R.g, id, PAR);
+  const Nbr n = make_nbr_fast(R.g, id, PAR);
   // FP32 draws: the replica's seed as key, its stream offset added to the
   // site index, the batch-wide drawing-phase counter (as for one lattice)
   PhaseArgs pa{R.beta, a.eps, a.upd, a.err, a.accept ? a.accept + R.site_off : nullptr, a.renorm,

@@ -82,6 +82,13 @@ __device__ __forceinline__ Nbr make_nbr_slice(const Geo& g, int s, int t, int pa
   return n;
 }
 
+// From the sublattice index with one division (the t-slice), the rest as in
+// make_nbr_slice; the same offsets as make_nbr.
+__device__ __forceinline__ Nbr make_nbr_fast(const Geo& g, int id, int parity) {
+  const int t = id / g.slice;
+  return make_nbr_slice(g, id - t * g.slice, t, parity);
+}
+
 __device__ __forceinline__ void finish_nbr(const Geo& g, int parity, Nbr& n) {
   n.q = ((n.t + n.x) & 1) ^ parity;
   // +y: a site with odd physical y moves to the next y' (wrapping), an even
