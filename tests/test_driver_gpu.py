@@ -130,12 +130,16 @@ def test_fp32_driver_run_with_report(tmp_path):
     assert any(n.startswith("Check_16_16_16_B_6.00_pmc_1") for n in os.listdir(tmp_path))
 
 
-def test_driver_resume_with_generator_state(tmp_path):
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_driver_resume_with_generator_state(tmp_path, precision):
+    # FP64: the MRG32k3a words; FP32: also the counter and key of its Philox draws
     from qcd_2d_gpu_b200.build import build_driver
 
     build_driver()
     common = ["--dt", 8, "--dx", 8, "--dy", 8, "--beta", 6, "--boundary", 0, "--N", 12, "--N-cor", 2, "--W", 3,
-              "--Nsave", 1, "--seed", 5, "--rng-state", 1, "--outdir", str(tmp_path)]
+              "--Nsave", 1, "--seed", 5, "--rng-state", 1, "--outdir", str(tmp_path), "--precision", precision]
+    if precision == "fp32":
+        common += ["--n-or", 2, "--renorm-every", 1]
     a = subprocess.run([DRIVER, *map(str, common + ["--N-term", 10])], capture_output=True, text=True, timeout=300)
     assert a.returncode == 0, a.stderr
     assert any(n.endswith("_rng.bin") for n in os.listdir(tmp_path))
