@@ -231,10 +231,12 @@ const char* qcd_status_string(int status);
  * whole batch is the six phase launches of one lattice, each covering every
  * replica, and a measurement is one launch writing every replica's
  * (energy, plaquette).  qcd_batch_run captures one measurement interval as a
- * CUDA graph and replays it.  Replica r draws from MRG32k3a streams
- * curand_init(seed_r, stream_offset_r + id, 0): with stream_offset 0 it
- * reproduces a single lattice of the same seed; giving replicas disjoint
- * offset blocks under one seed keeps every stream of the batch distinct.
+ * CUDA graph and replays it.  Replica r starts (and, in FP64, draws) from
+ * MRG32k3a streams curand_init(seed_r, stream_offset_r + id, 0); its FP32
+ * sweep draws from the Philox counters of site stream_offset_r + id under key
+ * seed_r.  With stream_offset 0 a replica reproduces a single lattice of the
+ * same seed; giving replicas disjoint offset blocks under one seed keeps every
+ * stream of the batch distinct.
  * ------------------------------------------------------------------------ */
 typedef struct qcd_replica {
   int lt, lx, ly;          /* even extents */
@@ -242,7 +244,7 @@ typedef struct qcd_replica {
   int boundary;            /* enum qcd_boundary */
   int hot;                 /* 1: hot start (rand_init2 / rand_init2_pcc), 0: cold */
   unsigned long long seed;
-  long long stream_offset; /* first MRG32k3a subsequence of this replica */
+  long long stream_offset; /* first MRG32k3a subsequence / Philox site counter of this replica */
 } qcd_replica;
 typedef struct qcd_batch qcd_batch;
 

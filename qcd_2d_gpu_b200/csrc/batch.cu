@@ -1,8 +1,9 @@
 // Batched replicas: many independent lattices of different size, coupling
 // and boundary condition advanced together.
 //
-// All replicas live in one link store and one RNG store (each replica's
-// planes contiguous, offsets in a device replica table).  One launch per
+// All replicas live in one link store and one MRG32k3a store (each
+// replica's planes contiguous, offsets in a device replica table; the FP32
+// sweep draws from Philox counters instead, as a single lattice does).  One launch per
 // checkerboard phase covers every replica: CTA c belongs to the replica whose
 // [cta_begin, cta_begin + ceil(V/2 / 256)) range holds c, so a sweep of the
 // whole batch is 6 launches (plus passes of over-relaxation) instead of

@@ -1,4 +1,6 @@
-// Per-site MRG32k3a streams, stored compactly.
+// Random numbers.  The FP64 sweep and every hot start draw from per-site
+// MRG32k3a streams, stored compactly; the FP32 sweep draws from the
+// counter-based Philox4x32-10 below and stores nothing.
 //
 // The reference keeps one curandStateMRG32k3a_t (48 B, AoS) per half-lattice
 // site and seeds stream id with curand_init(seed, id, 0) (lattice_setup.h:15-21,
