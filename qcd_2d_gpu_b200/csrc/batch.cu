@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(kBlock) batch_measure(BatchView B, double2* pa
   }
   double se, sp;
   block_sum2(e, pl * (1.0 / 3.0), &se, &sp);
-  __shared__ bool last_rep, last_all;
+  __shared__ bool last_rep;
   if (threadIdx.x == 0) {
     partials[blockIdx.x] = make_double2(se, sp);
     __threadfence();
@@ -200,16 +200,15 @@ __global__ void __launch_bounds__(kBlock) batch_measure(BatchView B, double2* pa
       const double scale = 1.0 / (2.0 * (double)R.g.vh);
       if (k < cap) series[(size_t)r * cap + k] = make_double2(sa * scale, sb * scale);
       rep_count[r] = 0u;
+      // the last replica to finish (every CTA of the launch done) moves the
+      // cursor: one atomic per replica, not one per CTA
+      __threadfence();
+      const bool last_all = atomicAdd(all_count, 1u) == (unsigned int)B.n - 1;
+      if (last_all) {
+        *all_count = 0u;
+        *cursor = k + 1;
+      }
     }
-  }
-  if (threadIdx.x == 0) {
-    __threadfence();
-    last_all = atomicAdd(all_count, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (last_all && threadIdx.x == 0) {
-    *all_count = 0u;
-    *cursor = k + 1;
   }
 }
 

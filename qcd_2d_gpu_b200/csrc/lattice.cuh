@@ -31,7 +31,16 @@ struct Geo {
   // exact when lyh^2 * lx < 2^32 (fastdiv = 1), otherwise a hardware division is used
   unsigned long long lyh_magic;
   int fastdiv;
+  // n / slice for any 32-bit n as the high word of n * slice_m (0: slice = 1)
+  unsigned long long slice_m;
 };
+
+// m = ceil(2^64 / d) for 2 <= d < 2^32 (0 for d = 1): floor(n * m / 2^64) =
+// floor(n / d) for every n < 2^32, because m * d - 2^64 < d
+__host__ __forceinline__ unsigned long long div_magic(unsigned long long d) { return ~0ull / d + 1; }
+__device__ __forceinline__ int div_by(unsigned int n, unsigned long long m) {
+  return m ? (int)__umul64hi((unsigned long long)n, m) : (int)n;
+}
 
 __host__ __forceinline__ Geo make_geo(int lt, int lx, int ly) {
   Geo g;
@@ -43,6 +52,7 @@ __host__ __forceinline__ Geo make_geo(int lt, int lx, int ly) {
   g.vh = g.slice * lt;
   g.lyh_magic = ((1ull << 32) + (unsigned long long)g.lyh - 1) / (unsigned long long)g.lyh;
   g.fastdiv = (unsigned long long)g.lyh * (unsigned long long)g.lyh * (unsigned long long)lx < (1ull << 32);
+  g.slice_m = div_magic((unsigned long long)g.slice);
   return g;
 }
 
@@ -82,10 +92,10 @@ __device__ __forceinline__ Nbr make_nbr_slice(const Geo& g, int s, int t, int pa
   return n;
 }
 
-// From the sublattice index with one division (the t-slice), the rest as in
+// From the sublattice index: the t-slice by a multiply-high, the rest as in
 // make_nbr_slice; the same offsets as make_nbr.
 __device__ __forceinline__ Nbr make_nbr_fast(const Geo& g, int id, int parity) {
-  const int t = id / g.slice;
+  const int t = div_by((unsigned int)id, g.slice_m);
   return make_nbr_slice(g, id - t * g.slice, t, parity);
 }
 

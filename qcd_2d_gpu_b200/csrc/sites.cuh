@@ -214,12 +214,12 @@ __host__ __device__ __forceinline__ unsigned int measure_blocks(long long vh) {
 
 // Energy and plaquette sums of the sites id = c*256 + tid, + nb*256, ... of
 // CTA c of nb (both parities): -(1 - P_xt) and 3 - sum of the three 1 - P.
-// One division finds the site's t-slice; the neighbours come from the
+// A multiply-high finds the site's t-slice; the neighbours come from the
 // slice position (multiply-high).
 template <class L, bool PMC>
 __device__ __forceinline__ void measure_sites(const L& links, const Geo& g, int c, int nb, double& e, double& pl) {
   for (int id = c * kBlock + threadIdx.x; id < g.vh; id += nb * kBlock) {
-    const int t = id / g.slice;
+    const int t = div_by((unsigned int)id, g.slice_m);
     const int s = id - t * g.slice;
     for (int p = 0; p < 2; p++) {
       const Nbr n = make_nbr_slice(g, s, t, p);
