@@ -1,0 +1,67 @@
+"""Parity with the reference's own kernels at the benchmark configurations.
+
+The golden fixtures (tests/golden) pin small lattices.  Here the reference's
+kernels (oracle/_ref/ref_harness, built from its sources for sm_100a) run at
+the full sizes of the benchmark configurations, and the FP64 path is
+compared with them field for field:
+  C2  32x32x64, PCC, beta 8, hot, Metropolis eps 0.2 upd 4 (the full config);
+  C3  the PMC heat-bath sweep at 96^3 (the 384^3 lattice's link dumps would
+      be 5.4 GB each; the sweep, its boundary and its streams are the same);
+  C5  128^3 periodic heat-bath from a cold start at beta 4.
+Heat-bath fields must agree bit for bit, Metropolis to the few ulp its
+proposal arithmetic contracts differently (with identical accept arrays);
+the energy and plaquette to 1e-13.
+"""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import qcd_2d_gpu_b200 as q
+from pyoracle import REF_HARNESS
+
+pytestmark = pytest.mark.gpu
+
+CONFIGS = [
+    # name, lt, lx, ly, algo, bc, hot, beta, eps, upd, seed, sweeps
+    ("C2_metro_pcc_32x32x64", 32, 32, 64, "metro", 1, 1, 8.0, 0.2, 4, 1234, 10),
+    ("C3_hb_pmc_hot_96", 96, 96, 96, "hb", 2, 1, 10.0, 0.1, 1, 1234, 10),
+    ("C5_hb_per_cold_128", 128, 128, 128, "hb", 0, 0, 4.0, 0.1, 1, 2026, 5),
+]
+
+
+@pytest.mark.parametrize("cfg", CONFIGS, ids=lambda c: c[0])
+def test_fp64_path_matches_the_reference_kernels_at_benchmark_sizes(cfg, tmp_path):
+    if not os.path.exists(REF_HARNESS):
+        pytest.skip("reference harness not built (needs the reference checkout at build time)")
+    name, lt, lx, ly, algo, bc, hot, beta, eps, upd, seed, sweeps = cfg
+    pre = str(tmp_path / name)
+    out = subprocess.run(
+        [REF_HARNESS, "run", "--lt", str(lt), "--lx", str(lx), "--ly", str(ly), "--algo", algo, "--bc", str(bc),
+         "--hot", str(hot), "--beta", repr(beta), "--eps", repr(eps), "--upd", str(upd), "--seed", str(seed),
+         "--sweeps", str(sweeps), "--dumps", str(sweeps), "--out", pre],
+        capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr
+    json.loads(out.stdout.strip().splitlines()[-1])
+    V = lt * lx * ly
+    ref = np.fromfile(f"{pre}_field_{sweeps}.bin", dtype=np.float64)
+    obs = np.fromfile(f"{pre}_obs.bin", dtype=np.float64).reshape(sweeps, 2)
+    acc = np.fromfile(f"{pre}_accept.bin", dtype=np.int32)
+    assert ref.size == V * 12 and acc.size == V
+
+    L = q.Lattice(lt, lx, ly, beta, algo=algo, boundary=bc, epsilon=eps, upd=upd, seed=seed)
+    L.init_hot() if hot else L.init_cold()
+    mine = []
+    for _ in range(sweeps):
+        L.sweep(1)
+        mine.append(L.measure())
+    field = L.store_config()
+    if algo == "metro":
+        assert np.abs(field - ref).max() <= 1e-12
+    else:
+        assert np.array_equal(field, ref), "heat-bath must be bit-identical"
+    assert np.abs(np.array(mine) - obs).max() <= 1e-13
+    assert np.array_equal(L.accept_counts(), acc)
+    L.close()
