@@ -458,6 +458,11 @@ def main():
             roofline["traffic"] = json.load(open(traffic_file)).get("phase32_or_bytes_per_launch")
         except Exception:
             pass
+    if roofline["traffic"]:
+        # the DRAM bytes a launch really moves (ncu) over its live time: how close
+        # the kernel runs to HBM for the traffic of its per-phase design
+        roofline["traffic_gbs"] = roofline["traffic"] / (or_launch_ms * 1e-3) / 1e9
+        roofline["traffic_frac"] = roofline["traffic_gbs"] / hbm
 
     # ---- end to end through the C ABI with host buffers -------------------
     # one host configuration in the reference's AoS FP64 layout is uploaded
