@@ -120,3 +120,22 @@ def test_fp32_seeds_give_different_chains():
         f.append(L.store_config())
         L.close()
     assert not np.array_equal(f[0], f[1])
+
+
+def test_headline_lattice_full_size_properties():
+    # the 384^3 PMC lattice of the benchmark: one sweep of 1 heat-bath + 3
+    # over-relaxation passes keeps every FP32 link on the group and gives a
+    # plaquette inside (0, 1); over-relaxation then conserves the total action
+    # (the plaquette average), while the energy observable (the x-t plaquettes
+    # alone) may move between planes
+    L = q.Lattice(384, 384, 384, 10.0, algo="hb", boundary="pmc", precision="fp32", n_or=3, renorm_every=1,
+                  seed=1234)
+    L.init_hot()
+    L.sweep(1)
+    assert abs(L.check_unitarity(2e-6) - 1.0) < 1e-6
+    _, p0 = L.measure()
+    assert 0.0 < p0 < 1.0
+    L.overrelax(2)
+    _, p1 = L.measure()
+    assert abs(p1 - p0) < 1e-6
+    L.close()
