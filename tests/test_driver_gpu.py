@@ -115,6 +115,22 @@ def test_driver_leaves_the_reference_files(r, tmp_path):
     if r[0] == "hb":
         compare_dirs(ra, rb, r[0])
         assert same_text("\n".join(stable_stdout(a.stdout)), "\n".join(stable_stdout(b.stdout)))
+    # read the configuration and thermalise further (readconf = 1): N_term
+    # accumulates into the _data.txt of the saved configuration
+    if r[0] == "hb":
+        rc, rd = tmp_path / "ref3", tmp_path / "ours3"
+        for src, dst in ((ref, rc), (ours, rd)):
+            dst.mkdir()
+            for name in os.listdir(src):
+                if name.startswith("Config_"):
+                    (dst / name).write_bytes((src / name).read_bytes())
+        a = subprocess.run([HARNESS, *map(str, harness_args(r, ["--readconf", 1, "--nsave", 3]))], cwd=rc,
+                           capture_output=True, text=True, timeout=300)
+        b = subprocess.run([DRIVER, "--algo", r[0], *map(str, knobs(r)), "--readconf", "1", "--nsave", "3",
+                            "--outdir", str(rd)], capture_output=True, text=True, timeout=300)
+        assert a.returncode == 0 and b.returncode == 0, (a.stderr, b.stderr)
+        compare_dirs(rc, rd, r[0])
+        assert same_text("\n".join(stable_stdout(a.stdout)), "\n".join(stable_stdout(b.stdout)))
 
 
 def test_fp32_driver_run_with_report(tmp_path):
