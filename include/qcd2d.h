@@ -324,17 +324,21 @@ int qcd_rng_tape(unsigned long long seed, long long first, int n_streams, int n_
  * a fixed array inside the library, present on every GPU that loads it until
  * the process exits.
  *
- * Limit: V/2 <= QCD_NOALLOC_MAX_HALF_SITES (V <= 8,388,608, e.g. 192^3);
- * larger lattices return QCD_ERR_UNSUPPORTED (and say so on stderr) — use
- * qcd_measure on a handle for those.
- * The first call on a device looks up the scratch array's device address
- * (with lazy module loading it also loads the library's kernels there); make
- * that first call before any stream capture.  All calls share the one
- * scratch array: calls that can overlap on the GPU (different streams, no
- * ordering between them) race and must not be issued.
+ * Limits: the scratch holds QCD_NOALLOC_MAX_BLOCKS partial sums (64 KB), which
+ * is the most CTAs any measurement launches, whatever the lattice size: the
+ * threads of a CTA stride over the sites.  The lattice itself is bounded only
+ * by the 32-bit site indices, V/2 <= QCD_NOALLOC_MAX_HALF_SITES (the same bound
+ * as qcd_create; 384^3 and larger fit); beyond it the call returns
+ * QCD_ERR_UNSUPPORTED (and says so on stderr) without touching the device.
+ * Every call looks up the scratch array's device address on the current
+ * device (no allocation; with lazy module loading the first call on a device
+ * also loads the library's kernels there): make that first call before any
+ * stream capture.  All calls share the one scratch array: calls that can
+ * overlap on the GPU (different streams, no ordering between them) race and
+ * must not be issued.
  * ------------------------------------------------------------------------ */
-#define QCD_NOALLOC_MAX_BLOCKS 16384
-#define QCD_NOALLOC_MAX_HALF_SITES (QCD_NOALLOC_MAX_BLOCKS * 256)
+#define QCD_NOALLOC_MAX_BLOCKS 4096
+#define QCD_NOALLOC_MAX_HALF_SITES 357913940 /* the largest V/2 below 2^31 / 6 */
 int qcd_measure_aos_noalloc(const double* phi_dev, int lt, int lx, int ly, int boundary,
                             double* out_dev, void* stream);
 

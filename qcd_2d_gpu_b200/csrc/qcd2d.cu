@@ -581,8 +581,9 @@ int qcd_create(const qcd_params* p, qcd_lattice** out) {
   if (p->precision != QCD_PREC_FP64 && p->precision != QCD_PREC_FP32) return QCD_ERR_INVALID;
   if (!(p->beta > 0.f) || p->upd < 0 || p->n_or < 0 || p->renorm_every < 0) return QCD_ERR_INVALID;
   if (p->algo == QCD_ALGO_METROPOLIS && !(p->epsilon > 0.f && p->epsilon < 1.f)) return QCD_ERR_INVALID;
+  if (0.5 * (double)p->lt * (double)p->lx * (double)p->ly >= (double)((1ll << 31) / 6))
+    return QCD_ERR_INVALID;  // 32-bit plane indices (checked in double: the product can overflow)
   long long V = (long long)p->lt * p->lx * p->ly;
-  if (V / 2 >= (1ll << 31) / 6) return QCD_ERR_INVALID;  // 32-bit plane indices
 
   qcd_lattice* h = new (std::nothrow) qcd_lattice();
   if (!h) return QCD_ERR_NOMEM;
@@ -856,7 +857,21 @@ int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
       }
   // the trials advance the lattice: save links, streams and counters, restore after
   const size_t rng_bytes = 6 * (size_t)h->g.vh * sizeof(uint32_t);
-  void *links_save = nullptr, *links2_save = nullptr, *rng_save = nullptr, *acc_save = nullptr;
+  // the backups are freed on every way out of this function (a failed
+  // allocation or copy returns early)
+  struct Backups {
+    void *links = nullptr, *links2 = nullptr, *rng = nullptr, *acc = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ~Backups() {
+      cudaFree(links);
+      cudaFree(links2);
+      cudaFree(rng);
+      cudaFree(acc);
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+    }
+  } bk;
+  void *&links_save = bk.links, *&links2_save = bk.links2, *&rng_save = bk.rng, *&acc_save = bk.acc;
   const size_t lb = h->p.precision == QCD_PREC_FP64 ? h->link_bytes / 2 : h->link_bytes;
   void* lp = h->p.precision == QCD_PREC_FP64 ? (void*)h->lo : (void*)h->q32;
   CUDA_OR_FAIL(h, cudaMalloc(&links_save, lb));
@@ -873,7 +888,7 @@ int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
   CUDA_OR_FAIL(h, cudaMemcpyAsync(&draws_save, h->draw_dev, sizeof(draws_save), cudaMemcpyDeviceToHost, h->stream));
   CUDA_OR_FAIL(h, cudaStreamSynchronize(h->stream));
   const int sched_save = h->sched, chunk_save = h->wave_chunk, chain_save = h->wave_chain, fronts_save = h->wave_fronts;
-  cudaEvent_t e0, e1;
+  cudaEvent_t &e0 = bk.e0, &e1 = bk.e1;
   CUDA_OR_FAIL(h, cudaEventCreate(&e0));
   CUDA_OR_FAIL(h, cudaEventCreate(&e1));
   int best = 0;
@@ -889,18 +904,12 @@ int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
     cand[i].ms_per_sweep = ms / sweeps_per_trial;
     if (rc == QCD_OK && cand[i].ms_per_sweep < cand[best].ms_per_sweep) best = (int)i;
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   // restore the lattice as it was
   cudaMemcpyAsync(lp, links_save, lb, cudaMemcpyDeviceToDevice, h->stream);
   if (links2_save) cudaMemcpyAsync(h->hi, links2_save, lb, cudaMemcpyDeviceToDevice, h->stream);
   cudaMemcpyAsync(h->rng, rng_save, rng_bytes, cudaMemcpyDeviceToDevice, h->stream);
   if (acc_save) cudaMemcpyAsync(h->accept, acc_save, (size_t)h->V * sizeof(int), cudaMemcpyDeviceToDevice, h->stream);
   cudaStreamSynchronize(h->stream);
-  cudaFree(links_save);
-  cudaFree(links2_save);
-  cudaFree(rng_save);
-  cudaFree(acc_save);
   cudaMemcpyAsync(h->draw_dev, &draws_save, sizeof(draws_save), cudaMemcpyHostToDevice, h->stream);
   cudaStreamSynchronize(h->stream);
   h->unit_passes = passes_save;
@@ -1137,36 +1146,31 @@ __device__ __forceinline__ Quat<double> ld64<LinksAoS>(const LinksAoS& links, in
 }  // namespace qcd
 
 // partial sums of at most QCD_NOALLOC_MAX_BLOCKS CTAs, then the arrival counter
+static_assert(kMeasureMaxBlocks <= QCD_NOALLOC_MAX_BLOCKS,
+              "a measurement may launch more CTAs than the no-allocation scratch has partial sums");
+static_assert((long long)QCD_NOALLOC_MAX_HALF_SITES * 6 < (1ll << 31), "32-bit plane indices");
 static constexpr size_t kNoAllocCounterOffset = (size_t)QCD_NOALLOC_MAX_BLOCKS * sizeof(double2);
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocCounterOffset + 256];
 
 namespace {
-std::mutex g_noalloc_mu;
-void* g_noalloc_addr[256];  // device address of g_noalloc_scratch, per device ordinal
-
 // Host code may not use g_noalloc_scratch itself (on the host it names a
-// stand-in, not device memory): look up its device address once per device,
-// with that device current.
+// stand-in, not device memory): look up its device address on the current
+// device at every call.  The lookup allocates nothing and is cheap once the
+// module is loaded; not caching it keeps the address right after a
+// cudaDeviceReset or under another context on the same device.
 int noalloc_scratch(void** out) {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 256) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
     cudaGetLastError();
+    int dev = -1;
+    cudaGetDevice(&dev);
+    cudaGetLastError();
+    fprintf(stderr, "qcd_measure_aos_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", dev,
+            cudaGetErrorString(e));
     return QCD_ERR_CUDA;
   }
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      cudaGetLastError();
-      fprintf(stderr, "qcd_measure_aos_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", dev,
-              cudaGetErrorString(e));
-      return QCD_ERR_CUDA;
-    }
-    g_noalloc_addr[dev] = p;
-  }
-  *out = g_noalloc_addr[dev];
+  *out = p;
   return QCD_OK;
 }
 }  // namespace
@@ -1177,15 +1181,16 @@ extern "C" int qcd_measure_aos_noalloc(const double* phi_dev, int lt, int lx, in
   if (lt < 2 || lx < 2 || ly < 2 || (lt & 1) || (lx & 1) || (ly & 1)) return QCD_ERR_INVALID;
   if (boundary < 0 || boundary > 2) return QCD_ERR_INVALID;
   if (((uintptr_t)phi_dev & 15) || ((uintptr_t)out_dev & 7)) return QCD_ERR_INVALID;
-  const long long vh = (long long)lt * lx * ly / 2;
-  const long long nb = (vh + kBlock - 1) / kBlock;
-  if (vh > QCD_NOALLOC_MAX_HALF_SITES || nb > QCD_NOALLOC_MAX_BLOCKS) {
+  // in double first: the product of three ints can overflow 64 bits
+  if (0.5 * (double)lt * (double)lx * (double)ly > (double)QCD_NOALLOC_MAX_HALF_SITES) {
     fprintf(stderr,
-            "qcd_measure_aos_noalloc: %dx%dx%d has V/2 = %lld sites, above the %d that its fixed "
-            "scratch holds; use qcd_measure on a handle instead\n",
-            lt, lx, ly, vh, QCD_NOALLOC_MAX_HALF_SITES);
+            "qcd_measure_aos_noalloc: %dx%dx%d has V/2 = %.0f sites, above the %d that 32-bit site "
+            "indices address\n",
+            lt, lx, ly, 0.5 * (double)lt * (double)lx * (double)ly, QCD_NOALLOC_MAX_HALF_SITES);
     return QCD_ERR_UNSUPPORTED;
   }
+  const long long vh = (long long)lt * lx * ly / 2;
+  if (measure_blocks(vh) > QCD_NOALLOC_MAX_BLOCKS) return QCD_ERR_UNSUPPORTED;  // excluded by the static_assert
   void* base = nullptr;
   int rc = noalloc_scratch(&base);
   if (rc) return rc;

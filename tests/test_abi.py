@@ -90,3 +90,15 @@ def test_defaults_match_reference_knobs():
     assert (p.lt, p.lx, p.ly) == (96, 96, 4)
     assert p.beta == 20.0 and abs(p.epsilon - 0.1) < 1e-7 and p.upd == 1
     assert p.algo == q.HEATBATH and p.boundary == q.PERIODIC and p.precision == q.FP64
+
+
+def test_noalloc_measurement_refuses_on_the_host():
+    # argument checks of qcd_measure_aos_noalloc happen before any CUDA call
+    # (the pointers below are never dereferenced)
+    lib = q.load_library()
+    fake = ctypes.c_void_p(256)
+    assert lib.qcd_measure_aos_noalloc(fake, 1024, 1024, 1024, 0, fake, None) == -7  # V/2 beyond 32-bit indices
+    assert lib.qcd_measure_aos_noalloc(fake, 1 << 30, 1 << 30, 1 << 30, 0, fake, None) == -7  # product overflows
+    assert lib.qcd_measure_aos_noalloc(fake, 8, 6, 5, 0, fake, None) == -1
+    assert lib.qcd_measure_aos_noalloc(fake, 8, 8, 8, -1, fake, None) == -1
+    assert lib.qcd_measure_aos_noalloc(fake, 8, 8, 8, 0, None, None) == -1

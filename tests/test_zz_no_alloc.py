@@ -78,11 +78,41 @@ def test_noalloc_allocates_nothing_after_first_call():
     L.close()
 
 
-def test_noalloc_rejects_lattices_beyond_its_scratch():
+def test_noalloc_large_lattice_matches_measure():
+    # 256^3 (V/2 = 8,388,608 sites): the scratch holds one partial per CTA and
+    # a measurement launches at most QCD_NOALLOC_MAX_BLOCKS CTAs whatever the
+    # size, so a lattice this large is measured too, with the sums of qcd_measure
+    import torch
+
     lib = q.load_library()
-    # 384^3 has V/2 = 28,311,552 > QCD_NOALLOC_MAX_HALF_SITES: refused on the host,
-    # before any device access (the pointers are never dereferenced)
+    n = 256
+    L = q.Lattice(n, n, n, 9.0, boundary=2, precision="fp64", seed=17)
+    L.init_hot()
+    phi = torch.empty(n ** 3 * 12, dtype=torch.float64, device="cuda")
+    assert lib.qcd_store_config_device(L.handle, _dev_ptr(phi)) == 0
+    e_ref, p_ref = L.measure()  # synchronises the handle's stream
+    out = torch.empty(2, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        out.fill_(float("nan"))
+        torch.cuda.synchronize()
+        assert lib.qcd_measure_aos_noalloc(_dev_ptr(phi), n, n, n, 2, _dev_ptr(out), None) == 0
+        torch.cuda.synchronize()
+        e, p = out.cpu().tolist()
+        assert abs(e - e_ref) <= TOL and abs(p - p_ref) <= TOL
+    L.close()
+    del phi
+
+
+def test_noalloc_refuses_bad_arguments_before_touching_the_device():
+    lib = q.load_library()
+    # every case below is refused on the host: the pointers are never dereferenced
     fake = ctypes.c_void_p(256)
-    assert lib.qcd_measure_aos_noalloc(fake, 384, 384, 384, 2, fake, None) == -7
+    # V/2 = 536,870,912 sites exceeds the 32-bit site indices (QCD_NOALLOC_MAX_HALF_SITES)
+    assert lib.qcd_measure_aos_noalloc(fake, 1024, 1024, 1024, 2, fake, None) == -7
+    # extents whose product overflows 64 bits
+    big = 1 << 30
+    assert lib.qcd_measure_aos_noalloc(fake, big, big, big, 0, fake, None) == -7
     assert lib.qcd_measure_aos_noalloc(fake, 8, 7, 8, 0, fake, None) == -1  # odd extent
+    assert lib.qcd_measure_aos_noalloc(fake, 8, 8, 8, 3, fake, None) == -1  # no such boundary
     assert lib.qcd_measure_aos_noalloc(None, 8, 8, 8, 0, fake, None) == -1
+    assert lib.qcd_measure_aos_noalloc(ctypes.c_void_p(264), 8, 8, 8, 0, fake, None) == -1  # not 16-B aligned
