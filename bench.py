@@ -189,28 +189,50 @@ def reference_batch_c4(harness):
             "sites": r["sites"]}
 
 
-def accuracy_scan(args, q, torch):
-    """FP32 + FP64 fix-ups against FP64 at 128^3, periodic and PMC, beta in
-    {4, 6, 8, 10, 12}: `--scan-sweeps` heat-bath sweeps from a cold start
-    (the first fifth discarded), a measurement every sweep; binned means and
-    errors, tau_int (Madras-Sokal, c = 6) and link updates/s per variant.
-    The FP64 path reproduces the reference's build bit for bit (the golden
-    tests), so its series stand for the reference's long runs; with
-    --impl reference the reference's own build is timed on the same runs."""
+def chain_stats(e, p):
+    """Binned means and errors (bins of ceil(4 tau_int), tau_int by the
+    Madras-Sokal window with c = 6) of an energy and a plaquette series."""
     import numpy as np
 
+    import qcd_2d_gpu_b200 as q
+
+    res = {}
+    for name, x in (("plaquette", p), ("energy", e)):
+        tau, w, dtau = q.tau_int(x, 6.0)
+        b = max(1, int(np.ceil(4 * tau)))
+        m, err = q.binned(x, b)
+        res[name] = {"mean": m, "err": err, "tau_int": tau, "dtau": dtau, "bin": b}
+    return res
+
+
+def compare_stats(a, b):
+    """|delta| and |delta| / sigma of the plaquette and energy means of two runs."""
+    import numpy as np
+
+    out = {}
+    for name in ("plaquette", "energy"):
+        d = abs(a[name]["mean"] - b[name]["mean"])
+        out[f"delta_{name}"] = d
+        out[f"delta_{name}_sigma"] = d / float(np.hypot(a[name]["err"], b[name]["err"]))
+    return out
+
+
+def scan_runs(q, torch, size, sweeps, bcs=(0, 2), betas=(4.0, 6.0, 8.0, 10.0, 12.0), seed=2026, emit=None):
+    """FP32 + FP64 fix-ups against FP64 at size^3: `sweeps` heat-bath sweeps
+    from a cold start (the first fifth discarded), a measurement every sweep;
+    binned means and errors, tau_int and link updates/s per variant.  The
+    FP64 path reproduces the reference's build bit for bit (the golden
+    tests), so its series stand for the reference's long runs."""
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    L3 = args.scan_size
-    sweeps = args.scan_sweeps
     therm = sweeps // 5
     out = []
-    for bc in (0, 2):
-        for beta in (4.0, 6.0, 8.0, 10.0, 12.0):
-            row = {"lattice": [L3] * 3, "boundary": bc, "beta": beta, "sweeps": sweeps, "discarded": therm}
+    for bc in bcs:
+        for beta in betas:
+            row = {"lattice": [size] * 3, "boundary": bc, "beta": beta, "sweeps": sweeps, "discarded": therm}
             for prec in ("fp64", "fp32"):
-                lat = q.Lattice(L3, L3, L3, beta, boundary=bc, precision=prec,
-                                renorm_every=1 if prec == "fp32" else 0, seed=2026)
+                lat = q.Lattice(size, size, size, beta, boundary=bc, precision=prec,
+                                renorm_every=1 if prec == "fp32" else 0, seed=seed)
                 lat.set_stream(stream.cuda_stream)
                 lat.init_cold()
                 lat.series_reserve(sweeps)
@@ -225,25 +247,89 @@ def accuracy_scan(args, q, torch):
                 e, p = lat.series_read(sweeps)
                 ms = e0.elapsed_time(e1)
                 lat.close()
-                res = {"link_updates_per_s": 3.0 * L3 ** 3 * sweeps / (ms * 1e-3)}
-                for name, x in (("plaquette", p[therm:]), ("energy", e[therm:])):
-                    tau, w, dtau = q.tau_int(x, 6.0)
-                    b = max(1, int(np.ceil(4 * tau)))
-                    m, err = q.binned(x, b)
-                    res[name] = {"mean": m, "err": err, "tau_int": tau, "dtau": dtau, "bin": b}
+                res = chain_stats(e[therm:], p[therm:])
+                res["link_updates_per_s"] = 3.0 * size ** 3 * sweeps / (ms * 1e-3)
                 row[prec] = res
-            for name in ("plaquette", "energy"):
-                a, b = row["fp64"][name], row["fp32"][name]
-                d = abs(a["mean"] - b["mean"])
-                row[f"delta_{name}"] = d
-                row[f"delta_{name}_sigma"] = d / float(np.hypot(a["err"], b["err"]))
+            row.update(compare_stats(row["fp64"], row["fp32"]))
             out.append(row)
-            print(json.dumps(row), flush=True)
+            if emit:
+                emit(row)
+    torch.cuda.set_stream(torch.cuda.default_stream())
+    return out
+
+
+def accuracy_scan(args, q, torch):
+    """The accuracy scan (C5): 128^3, periodic and PMC, beta in {4, 6, 8, 10,
+    12}, FP32 + FP64 fix-ups against FP64 (see scan_runs)."""
+    out = scan_runs(q, torch, args.scan_size, args.scan_sweeps, emit=lambda r: print(json.dumps(r), flush=True))
     n2 = sum(1 for r in out for k in ("plaquette", "energy") if r[f"delta_{k}_sigma"] <= 2.0)
     print(json.dumps({"summary": f"{n2} of {2 * len(out)} FP32-vs-FP64 comparisons within 2 sigma",
                       "max_delta_plaquette": max(r["delta_plaquette"] for r in out),
                       "max_delta_energy": max(r["delta_energy"] for r in out)}))
     return 0
+
+
+def c3_accuracy(q, torch, size=LT, n_term=300, n_meas=100, n_cor=2, seed=1234):
+    """The benchmark's own workload at matched accuracy: the 384^3 PMC lattice
+    at beta 10 from the same hot start, sweep = 1 heat-bath + 3
+    over-relaxation passes, run in FP32 + FP64 fix-ups (links re-projected
+    every sweep) and in FP64 (re-projected every 100 sweeps like the
+    reference's run loop), each with n_term thermalisation sweeps, then n_meas
+    measurements n_cor sweeps apart; binned means and errors and tau_int
+    of the plaquette and the energy, and |delta| / sigma between the two."""
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    row = {"lattice": [size] * 3, "boundary": "pmc", "beta": BETA, "n_or": N_OR, "n_term": n_term, "n_meas": n_meas,
+           "n_cor": n_cor, "start": "hot", "seed": seed}
+    for prec in ("fp32", "fp64"):
+        lat = q.Lattice(size, size, size, BETA, algo="hb", boundary="pmc", precision=prec, n_or=N_OR,
+                        renorm_every=1 if prec == "fp32" else 100, seed=seed)
+        lat.set_stream(stream.cuda_stream)
+        lat.init_hot()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        lat.sweep(n_term)
+        lat.series_reserve(n_meas)
+        for i in range(n_meas):
+            lat.sweep(n_cor)
+            lat.measure_into_series(i)
+        e1.record(stream)
+        e, p = lat.series_read(n_meas)
+        ms = e0.elapsed_time(e1)
+        lat.close()
+        res = chain_stats(e, p)
+        res["link_updates_per_s"] = 3.0 * size ** 3 * (1 + N_OR) * (n_term + n_meas * n_cor) / (ms * 1e-3)
+        res["seconds"] = ms * 1e-3
+        row[prec] = res
+    row.update(compare_stats(row["fp64"], row["fp32"]))
+    torch.cuda.set_stream(torch.cuda.default_stream())
+    return row
+
+
+def same_work(q, torch, stream, precision, steps, warmup=3, rank=0):
+    """The reference arm's exact workload on our kernels: the 384^3 PMC
+    lattice from a hot start, heat-bath sweeps only (the reference's
+    mc_up_pmc, mc_updates_pmc.h:249-257), one measurement every N_COR sweeps
+    (en_av, observables.h:99-141); link updates/s over `steps` measurement
+    intervals."""
+    L = q.Lattice(LT, LX, LY, BETA, algo="hb", boundary="pmc", precision=precision, n_or=0,
+                  renorm_every=1 if precision == "fp32" else 0, seed=1234 + rank)
+    L.set_stream(stream.cuda_stream)
+    L.init_hot()
+    L.series_reserve(1)
+    for _ in range(warmup):
+        L.sweep(N_COR)
+        L.measure_into_series(0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        L.sweep(N_COR)
+        L.measure_into_series(0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    L.close()
+    ms = e0.elapsed_time(e1)
+    return 3.0 * LT * LX * LY * N_COR * steps / (ms * 1e-3), ms / steps
 
 
 def dist_env():
@@ -303,9 +389,13 @@ def reference_arm(args, ws, rank):
                                f"has no PMC over-relaxation and no FP32 path), FP64, measure every {N_COR} "
                                "sweeps", "lattice": [LT, LX, LY], "boundary": "pmc", "precision": "fp64",
                    "n_or": 0, "n_cor": N_COR, "l2": "inputs larger than L2 (5.4 GB link field)"},
-        "cpu_baseline": {"value": ups, "unit": "link updates/s", "cores": 1, "kind": "reference",
-                         "sample": f"reference kernels built for sm_100a on the B200, {sweeps} sweeps timed "
-                                   "with CUDA events (the reference has no CPU implementation)"},
+        # the reference's implementation of the path is CUDA only: this line
+        # times its kernels on the B200, and no CPU number belongs to it (the
+        # CPU transcription of its sweep is our arm's cpu_baseline)
+        "cpu_baseline": {"value": None, "unit": "link updates/s", "cores": 0, "kind": "reference",
+                         "sample": f"none: the reference has no CPU implementation; this arm ran its kernels "
+                                   f"(mc_up_pmc + en_av) built for sm_100a on the B200, {sweeps} sweeps timed "
+                                   "with CUDA events"},
         "e2e": {"value": ups, "unit": "link updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "heatbath_pass_link_updates_per_s": 3.0 * LT * LX * LY / (r["ms_per_sweep"] * 1e-3),
         "reference_raw": r,
@@ -324,7 +414,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-replica measurement")
     ap.add_argument("--lattice", type=int, nargs=3, default=None, help="override (testing only)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "accuracy"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "accuracy", "c3-accuracy"])
     ap.add_argument("--schedule", default="auto", choices=["auto", "phases", "wavefront"])
     ap.add_argument("--wave-tuning", type=int, nargs=3, default=None, metavar=("CHUNK", "PASSES", "FRONTS"))
     ap.add_argument("--scan-size", type=int, default=128)
@@ -345,6 +435,13 @@ def main():
         import qcd_2d_gpu_b200 as q
 
         return accuracy_scan(args, q, torch)
+    if args.workload == "c3-accuracy":
+        import torch
+
+        import qcd_2d_gpu_b200 as q
+
+        print(json.dumps(c3_accuracy(q, torch, size=LT)))
+        return 0
     if args.impl == "reference":
         return reference_arm(args, ws, rank)
 
@@ -464,6 +561,15 @@ def main():
         roofline["traffic_gbs"] = roofline["traffic"] / (or_launch_ms * 1e-3) / 1e9
         roofline["traffic_frac"] = roofline["traffic_gbs"] / hbm
 
+    # ---- the reference arm's workload on our kernels ------------------------
+    # (heat-bath only, a measurement every N_COR sweeps): the like-for-like
+    # rates against the reference arm's line, in both precisions
+    sw = {"workload": f"{LT}x{LX}x{LY} PMC hot, heat-bath sweeps only, one measurement every {N_COR} sweeps "
+                      "(the reference arm's workload)", "steps": args.steps}
+    for prec in ("fp64", "fp32"):
+        rate, ms_s = same_work(q, torch, stream, prec, args.steps, rank=rank)
+        sw[prec] = {"link_updates_per_s": rate, "ms_per_step": ms_s}
+
     # ---- end to end through the C ABI with host buffers -------------------
     # one host configuration in the reference's AoS FP64 layout is uploaded
     # (pinned host -> device, converted to FP32 SoA) at the start of the timed
@@ -528,6 +634,7 @@ def main():
             # one heat-bath pass alone (timed live above): the rate comparable
             # with the reference's heat-bath-only sweep
             "heatbath_pass_link_updates_per_s": 3.0 * V / (hb_pass_ms * 1e-3),
+            "same_work_as_reference": sw,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "link updates/s",

@@ -561,3 +561,247 @@ int ora_get_threads(void) {
   return 1;
 #endif
 }
+
+/* ================================================ FP32 links + FP64 fix-ups
+ * Restatement of the library's own FP32 update path, the checker of its FP32
+ * kernels (heatbath_fast, metropolis_fast, overrelax_fast and renorm_fast in
+ * qcd_2d_gpu_b200/csrc/updates.cuh, site32 in csrc/sites.cuh).  The reference
+ * has FP64 links only; its algorithm (mc_updates.h:7-64,109-115 and the PCC/PMC
+ * masks of mc_updates_pcc.h / mc_updates_pmc.h) is kept step for step, with the
+ * arithmetic in float except for the fix-ups done in double: the heat-bath
+ * accept test, the length of the new link's spatial part, the Metropolis
+ * action change and accept test, and the re-projection.
+ *
+ * The field holds float values (as doubles): links are read as floats and
+ * written back as (double)float.  Draws come from Philox4x32-10 (Salmon,
+ * Moraes, Dror, Shaw, SC'11) with counter (site, block, phase lo, phase hi)
+ * and key (seed lo, seed hi), consumed word by word.  Host libm stands in for
+ * the GPU's hardware cos/log/sincos (absolute error ~2^-21 there), so a
+ * heat-bath accept decision can come out differently in rare cases; the
+ * checks compare at float tolerance and count such sites. */
+typedef struct {
+  float w, x, y, z;
+} fquat;
+
+static inline fquat f_ld(const double* p) { return (fquat){(float)p[0], (float)p[1], (float)p[2], (float)p[3]}; }
+static inline void f_st(double* p, fquat u) {
+  p[0] = u.w;
+  p[1] = u.x;
+  p[2] = u.y;
+  p[3] = u.z;
+}
+static inline fquat f_add(fquat a, fquat b) { return (fquat){a.w + b.w, a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline fquat f_mul(fquat a, fquat b) { /* su2.h:50-55 in float */
+  fquat c;
+  c.w = a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z;
+  c.x = a.x * b.w + a.w * b.x + a.y * b.z - a.z * b.y;
+  c.y = a.y * b.w + a.z * b.x + a.w * b.y - a.x * b.z;
+  c.z = a.z * b.w - a.y * b.x + a.w * b.z + a.x * b.y;
+  return c;
+}
+static inline fquat f_mul_bd(fquat a, fquat b) { /* su2.h:56-61 */
+  fquat c;
+  c.w = a.w * b.w + a.x * b.x + a.y * b.y + a.z * b.z;
+  c.x = a.x * b.w - a.w * b.x - a.y * b.z + a.z * b.y;
+  c.y = a.y * b.w - a.z * b.x - a.w * b.y + a.x * b.z;
+  c.z = a.z * b.w + a.y * b.x - a.w * b.z - a.x * b.y;
+  return c;
+}
+static inline fquat f_mul_ad(fquat a, fquat b) { /* su2.h:62-67 */
+  fquat c;
+  c.w = a.w * b.w + a.x * b.x + a.y * b.y + a.z * b.z;
+  c.x = -a.x * b.w + a.w * b.x - a.y * b.z + a.z * b.y;
+  c.y = -a.y * b.w - a.z * b.x + a.w * b.y + a.x * b.z;
+  c.z = -a.z * b.w + a.y * b.x + a.w * b.z - a.x * b.y;
+  return c;
+}
+static inline fquat f_mul_adbd(fquat a, fquat b) { /* su2.h:68-73 */
+  fquat c;
+  c.w = a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z;
+  c.x = -a.x * b.w - a.w * b.x + a.y * b.z - a.z * b.y;
+  c.y = -a.y * b.w + a.z * b.x - a.w * b.y - a.x * b.z;
+  c.z = -a.z * b.w - a.y * b.x - a.w * b.z + a.x * b.y;
+  return c;
+}
+static inline float f_det(fquat a) { return a.w * a.w + a.x * a.x + a.y * a.y + a.z * a.z; }
+static inline fquat f_scale(fquat a, float s) { return (fquat){a.w * s, a.x * s, a.y * s, a.z * s}; }
+
+/* Philox4x32-10: ten rounds of two 32 x 32 -> 64-bit products with the
+ * multipliers 0xD2511F53 and 0xCD9E8D57, the round key bumped by the Weyl
+ * increments 0x9E3779B9 and 0xBB67AE85 between rounds. */
+static void philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  uint32_t x0 = ctr[0], x1 = ctr[1], x2 = ctr[2], x3 = ctr[3], k0 = key[0], k1 = key[1];
+  for (int r = 0; r < 10; r++) {
+    if (r) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    uint64_t p0 = (uint64_t)0xD2511F53u * x0, p1 = (uint64_t)0xCD9E8D57u * x2;
+    uint32_t y0 = (uint32_t)(p1 >> 32) ^ x1 ^ k0, y2 = (uint32_t)(p0 >> 32) ^ x3 ^ k1;
+    x1 = (uint32_t)p1;
+    x3 = (uint32_t)p0;
+    x0 = y0;
+    x2 = y2;
+  }
+  out[0] = x0;
+  out[1] = x1;
+  out[2] = x2;
+  out[3] = x3;
+}
+
+typedef struct {
+  uint32_t ctr[4], key[2], buf[4];
+  int left, pos;
+} pstream;
+
+static inline void ps_init(pstream* s, unsigned long long seed, uint32_t site, unsigned long long phase) {
+  s->key[0] = (uint32_t)seed;
+  s->key[1] = (uint32_t)(seed >> 32);
+  s->ctr[0] = site;
+  s->ctr[1] = 0;
+  s->ctr[2] = (uint32_t)phase;
+  s->ctr[3] = (uint32_t)(phase >> 32);
+  s->left = 0;
+  s->pos = 0;
+}
+static inline uint32_t ps_next(pstream* s) {
+  if (s->left == 0) {
+    philox4x32_10(s->ctr, s->key, s->buf);
+    s->ctr[1]++;
+    s->left = 4;
+    s->pos = 0;
+  }
+  s->left--;
+  return s->buf[s->pos++];
+}
+/* (k + 1) / 2^24 of the top 24 bits: a float in (0, 1] */
+static inline float ps_uniform(pstream* s) { return (float)((ps_next(s) >> 8) + 1u) * 5.9604644775390625e-8f; }
+/* (k + 1) / 2^53 of 53 bits of two words: a double in (0, 1] */
+static inline double ps_uniform_double(pstream* s) {
+  uint64_t hi = ps_next(s), lo = ps_next(s);
+  return (double)(((hi << 21) | (lo >> 11)) + 1ull) * 1.1102230246251565e-16;
+}
+
+static fquat staples32(const ora_lattice* h, int mu, int par, int id, const nbr_t* n) {
+  const int o = par ^ 1;
+  const int nus[3][2] = {{1, 2}, {0, 2}, {0, 1}};
+  fquat A = {0, 0, 0, 0};
+  for (int k = 0; k < 2; k++) {
+    int nu = nus[mu][k];
+    int pmc = h->p.boundary == 2 && nu == 0;
+    int drop_fwd = pmc && n->yq == h->lyh - 1 && n->q == 1;
+    int drop_bwd = pmc && n->yq == 0 && n->q == 0;
+    if (!drop_fwd) {
+      fquat a = f_ld(L(h, o, id + plus(n, mu), nu));
+      fquat b = f_ld(L(h, o, id + plus(n, nu), mu));
+      fquat c = f_ld(L(h, par, id, nu));
+      A = f_add(A, f_mul_bd(f_mul_bd(a, b), c));
+    }
+    if (!drop_bwd) {
+      int m = id + minus(n, nu);
+      fquat a = f_ld(L(h, par, m + plus(n, mu), nu));
+      fquat b = f_ld(L(h, o, m, mu));
+      fquat c = f_ld(L(h, o, m, nu));
+      A = f_add(A, f_mul(f_mul_adbd(a, b), c));
+    }
+  }
+  return A;
+}
+
+/* Kennedy-Pendleton (mc_updates.h:43-64) in float; the accept test
+ * (1 - lf is within an ulp of 1 for a large coupling) and the length
+ * n = 2 sqrt(lf (1 - lf)) of the spatial part in double */
+static fquat heat_bath32(fquat A, float beta, pstream* st, int* tries_out) {
+  float det = f_det(A), rinv = 1.0f / sqrtf(det), a = det * rinv;
+  A = f_scale(A, rinv);
+  float inv = 0.5f / (a * beta), lf = 0.f, aux;
+  int tries = 0;
+  for (tries = 1; tries <= 4096; tries++) {
+    float r0 = ps_uniform(st), r1 = ps_uniform(st), r2 = ps_uniform(st);
+    float c = -cosf(6.2831853f * (r1 - 0.5f));
+    lf = -(logf(r0) + c * c * logf(r2)) * inv;
+    aux = 1.f - ps_uniform(st);
+    if (!((double)aux * aux > 1.0 - (double)lf)) break;
+  }
+  *tries_out = tries;
+  double lfd = lf;
+  float x0 = (float)(1.0 - 2.0 * lfd);
+  float nrm = (float)(2.0 * sqrt(lfd * (1.0 - lfd)));
+  float ct = 2.f * ps_uniform(st) - 1.f;
+  float ang = 6.2831853f * (ps_uniform(st) - 0.5f);
+  float sp = sinf(ang), cp = cosf(ang);
+  float stt = sqrtf(fmaxf(0.f, 1.f - ct * ct));
+  fquat X = {x0, nrm * ct, -nrm * stt * cp, -nrm * stt * sp};
+  return f_mul_bd(X, A);
+}
+
+/* mc_updates.h:16-36 in float, the action change and the accept test
+ * (mc_updates.h:7-15) in double */
+static int metropolis32(fquat* U, fquat A, float beta, float eps, int upd, pstream* st) {
+  int acc = 0;
+  const float r0 = sqrtf(1.f - eps * eps);
+  for (int hit = 0; hit < upd; hit++) {
+    float r1 = ps_uniform(st) - 0.5f, r2 = ps_uniform(st) - 0.5f, r3 = ps_uniform(st) - 0.5f;
+    float sc = eps * (1.0f / sqrtf(r1 * r1 + r2 * r2 + r3 * r3));
+    fquat r = {r0, sc * r1, sc * r2, sc * r3};
+    fquat Un = f_mul(r, *U);
+    fquat dU = {Un.w - U->w, Un.x - U->x, Un.y - U->y, Un.z - U->z};
+    float retr = dU.w * A.w - dU.x * A.x - dU.y * A.y - dU.z * A.z;
+    double s = -(double)beta * (double)retr;
+    int ok = s < 0 ? 1 : metropolis_accept(s, ps_uniform_double(st));
+    if (ok) {
+      *U = Un;
+      acc++;
+    }
+  }
+  return acc;
+}
+
+/* mc_updates.h:109-115 in float */
+static fquat over_relaxation32(fquat A, fquat U) {
+  A = f_scale(A, 1.0f / sqrtf(f_det(A)));
+  return f_mul_ad(A, f_mul_adbd(U, A));
+}
+
+/* re-projection with the norm taken in double */
+static fquat renorm32(fquat u) {
+  double d = (double)u.w * u.w + (double)u.x * u.x + (double)u.y * u.y + (double)u.z * u.z;
+  double inv = 1.0 / sqrt(d);
+  return (fquat){(float)(u.w * inv), (float)(u.x * inv), (float)(u.y * inv), (float)(u.z * inv)};
+}
+
+int ora_phase32(ora_lattice* h, int k, int kind, unsigned long long key, unsigned long long phase, int renorm,
+                int* hb_tries) {
+  if (!h || k < 0 || k > 5 || kind < 0 || kind > 2) return ORA_ERR_INVALID;
+  const int mu = k / 2, par = k % 2;
+  const float beta = h->p.beta;
+#pragma omp parallel for schedule(static)
+  for (int id = 0; id < h->vh; id++) {
+    nbr_t n = nbr(h, id, par);
+    if (h->p.boundary == 1 && mu != 0 && n.yq == 0 && n.q == 0) continue;
+    fquat A = staples32(h, mu, par, id, &n);
+    double* u = L(h, par, id, mu);
+    size_t site = (size_t)par * h->vh + id;
+    fquat U;
+    if (kind == 1) {
+      pstream st;
+      ps_init(&st, key, (uint32_t)id, phase);
+      int tries = 0;
+      U = heat_bath32(A, beta, &st, &tries);
+      if (hb_tries) hb_tries[site] = tries;
+      h->accept[site] += 1;
+    } else if (kind == 0) {
+      pstream st;
+      ps_init(&st, key, (uint32_t)id, phase);
+      U = f_ld(u);
+      h->accept[site] += metropolis32(&U, A, beta, h->p.epsilon, h->p.upd, &st);
+    } else {
+      U = over_relaxation32(A, f_ld(u));
+      h->accept[site] += 1;
+    }
+    f_st(u, renorm ? renorm32(U) : U);
+  }
+  return h->err;
+}
+
+void ora_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) { philox4x32_10(ctr, key, out); }

@@ -59,6 +59,15 @@ int ora_sweep(ora_lattice* h, int n);
 int ora_overrelax(ora_lattice* h, int n);
 int ora_normalize(ora_lattice* h);
 int ora_measure(ora_lattice* h, double* energy, double* plaquette);
+/* One phase of the library's FP32 path (float links, FP64 fix-ups), the
+   checker of its FP32 kernels: kind as for ora_phase; draws from Philox4x32-10
+   with counter (site id, block, phase lo, phase hi) and key (key lo, key hi);
+   renorm re-projects each updated link.  With hb_tries (V ints, reference
+   site order) the heat-bath stores the rejection-loop trips of each site. */
+/* one Philox4x32-10 block of the FP32 restatement (for pinning it) */
+void ora_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+int ora_phase32(ora_lattice* h, int k, int kind, unsigned long long key, unsigned long long phase, int renorm,
+                int* hb_tries);
 const double* ora_field(const ora_lattice* h);
 const int* ora_accept(const ora_lattice* h);
 long long ora_volume(const ora_lattice* h);

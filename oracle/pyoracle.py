@@ -77,6 +77,11 @@ def load() -> ctypes.CDLL:
     lib.ora_volume.argtypes = [P]
     lib.ora_max_draws.restype = ctypes.c_longlong
     lib.ora_max_draws.argtypes = [P]
+    lib.ora_phase32.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int,
+                                P]
+    lib.ora_phase32.restype = ctypes.c_int
+    lib.ora_philox4x32.argtypes = [P, P, P]
+    lib.ora_philox4x32.restype = None
     lib.ora_set_threads.argtypes = [ctypes.c_int]
     lib.ora_set_threads.restype = ctypes.c_int
     lib.ora_get_threads.restype = ctypes.c_int
@@ -139,6 +144,23 @@ class Oracle:
     def sweep(self, n=1):
         self._rc(self.lib.ora_sweep(self.h, n), "sweep")
 
+    def phase32(self, k, kind, key=0, phase=0, renorm=False, hb_tries=None):
+        """One phase of the FP32 path (float links, FP64 fix-ups, Philox draws
+        of counter (site, block, phase) under `key`); hb_tries, an int32 array
+        of V entries, receives the heat-bath rejection-loop trips per site."""
+        t = None
+        if hb_tries is not None:
+            assert hb_tries.dtype == np.int32 and hb_tries.size == self.V and hb_tries.flags.c_contiguous
+            t = ctypes.c_void_p(hb_tries.ctypes.data)
+        self._rc(self.lib.ora_phase32(self.h, k, kind, key, phase, int(renorm), t), f"phase32 {k}")
+
+    def sweep32(self, n=1, kind=1, key=0, phase=0, renorm_last=False):
+        """n passes of the six phases in the FP32 path, drawing phases
+        phase, phase + 1, ... (six per heat-bath or Metropolis pass)."""
+        for s in range(n):
+            for k in range(6):
+                self.phase32(k, kind, key, phase + 6 * s + k, renorm_last and s == n - 1)
+
     def overrelax(self, n=1):
         self._rc(self.lib.ora_overrelax(self.h, n), "overrelax")
 
@@ -162,3 +184,13 @@ class Oracle:
 
 def set_threads(n: int) -> int:
     return load().ora_set_threads(n)
+
+
+def philox4x32(ctr, key) -> np.ndarray:
+    """One Philox4x32-10 block of the oracle's FP32 restatement."""
+    lib = load()
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.empty(4, dtype=np.uint32)
+    lib.ora_philox4x32(ctypes.c_void_p(c.ctypes.data), ctypes.c_void_p(k.ctypes.data), ctypes.c_void_p(out.ctypes.data))
+    return out

@@ -512,6 +512,18 @@ int run_passes(qcd_lattice* h, const PassSpec* ps, int np) {
   return QCD_OK;
 }
 
+// The MRG32k3a streams, seeded curand_init(seed, id, 0) on first use: at
+// create for FP64 lattices, at the first hot start or generator checkpoint
+// for FP32 ones (whose sweep draws from the counter-based stream).  Seeding
+// late gives the same words as seeding at create.
+int ensure_rng(qcd_lattice* h) {
+  if (h->rng) return QCD_OK;
+  CUDA_OR_FAIL(h, cudaMalloc(&h->rng, 6 * (size_t)h->g.vh * sizeof(uint32_t)));
+  rng_setup<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(rngs(h), h->p.seed, h->g.vh);
+  LAUNCH_CHECK(h);
+  return QCD_OK;
+}
+
 void release(qcd_lattice* h) {
   cudaFree(h->lo);
   cudaFree(h->hi);
@@ -610,7 +622,11 @@ int qcd_create(const qcd_params* p, qcd_lattice** out) {
     h->link_bytes = 6 * vh * sizeof(float4);
     if (rc == QCD_OK) step(cudaMalloc(&h->q32, 6 * vh * sizeof(float4)), "cudaMalloc(links)");
   }
-  if (rc == QCD_OK) step(cudaMalloc(&h->rng, 6 * vh * sizeof(uint32_t)), "cudaMalloc(rng)");
+  // the FP64 sweep draws from the stored MRG32k3a streams at every update; an
+  // FP32 lattice needs them only for a hot start or a generator checkpoint,
+  // so it seeds them on first use (ensure_rng)
+  if (rc == QCD_OK && p->precision == QCD_PREC_FP64)
+    step(cudaMalloc(&h->rng, 6 * vh * sizeof(uint32_t)), "cudaMalloc(rng)");
   if (rc == QCD_OK && p->algo == QCD_ALGO_METROPOLIS) {
     step(cudaMalloc(&h->accept, 2 * vh * sizeof(int)), "cudaMalloc(accept)");
     if (rc == QCD_OK) step(cudaMemsetAsync(h->accept, 0, 2 * vh * sizeof(int), h->stream), "memset");
@@ -625,7 +641,7 @@ int qcd_create(const qcd_params* p, qcd_lattice** out) {
   if (rc == QCD_OK) step(cudaMallocHost(&h->result_host, 4 * sizeof(double)), "cudaMallocHost");
   if (rc == QCD_OK) step(cudaMemsetAsync(h->counter, 0, sizeof(unsigned int), h->stream), "memset");
   if (rc == QCD_OK) step(cudaMemsetAsync(h->err, 0, sizeof(int), h->stream), "memset");
-  if (rc == QCD_OK) {
+  if (rc == QCD_OK && h->rng) {
     rng_setup<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(rngs(h), p->seed, h->g.vh);
     step(cudaGetLastError(), "rng_setup");
   }
@@ -669,6 +685,8 @@ int qcd_init_cold(qcd_lattice* h) {
 
 int qcd_init_hot(qcd_lattice* h) {
   if (!h) return QCD_ERR_INVALID;
+  int rc = ensure_rng(h);
+  if (rc) return rc;
   const int pcc = h->p.boundary == QCD_BC_PCC;
   if (h->p.precision == QCD_PREC_FP64)
     init_hot<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(links64(h), rngs(h), h->g, pcc);
@@ -876,11 +894,11 @@ int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
   void* lp = h->p.precision == QCD_PREC_FP64 ? (void*)h->lo : (void*)h->q32;
   CUDA_OR_FAIL(h, cudaMalloc(&links_save, lb));
   if (h->p.precision == QCD_PREC_FP64) CUDA_OR_FAIL(h, cudaMalloc(&links2_save, lb));
-  CUDA_OR_FAIL(h, cudaMalloc(&rng_save, rng_bytes));
+  if (h->rng) CUDA_OR_FAIL(h, cudaMalloc(&rng_save, rng_bytes));
   if (h->accept) CUDA_OR_FAIL(h, cudaMalloc(&acc_save, (size_t)h->V * sizeof(int)));
   CUDA_OR_FAIL(h, cudaMemcpyAsync(links_save, lp, lb, cudaMemcpyDeviceToDevice, h->stream));
   if (links2_save) CUDA_OR_FAIL(h, cudaMemcpyAsync(links2_save, h->hi, lb, cudaMemcpyDeviceToDevice, h->stream));
-  CUDA_OR_FAIL(h, cudaMemcpyAsync(rng_save, h->rng, rng_bytes, cudaMemcpyDeviceToDevice, h->stream));
+  if (rng_save) CUDA_OR_FAIL(h, cudaMemcpyAsync(rng_save, h->rng, rng_bytes, cudaMemcpyDeviceToDevice, h->stream));
   if (acc_save)
     CUDA_OR_FAIL(h, cudaMemcpyAsync(acc_save, h->accept, (size_t)h->V * sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
   const long long passes_save = h->unit_passes, sweeps_save = h->sweeps_done;
@@ -907,7 +925,7 @@ int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
   // restore the lattice as it was
   cudaMemcpyAsync(lp, links_save, lb, cudaMemcpyDeviceToDevice, h->stream);
   if (links2_save) cudaMemcpyAsync(h->hi, links2_save, lb, cudaMemcpyDeviceToDevice, h->stream);
-  cudaMemcpyAsync(h->rng, rng_save, rng_bytes, cudaMemcpyDeviceToDevice, h->stream);
+  if (rng_save) cudaMemcpyAsync(h->rng, rng_save, rng_bytes, cudaMemcpyDeviceToDevice, h->stream);
   if (acc_save) cudaMemcpyAsync(h->accept, acc_save, (size_t)h->V * sizeof(int), cudaMemcpyDeviceToDevice, h->stream);
   cudaStreamSynchronize(h->stream);
   cudaMemcpyAsync(h->draw_dev, &draws_save, sizeof(draws_save), cudaMemcpyHostToDevice, h->stream);
@@ -1056,6 +1074,8 @@ long long qcd_rng_words(const qcd_lattice* h) { return h ? 6 * (long long)h->g.v
 
 int qcd_store_rng(qcd_lattice* h, uint32_t* host_out) {
   if (!h || !host_out) return QCD_ERR_INVALID;
+  int rc0 = ensure_rng(h);
+  if (rc0) return rc0;
   const size_t n = 6 * (size_t)h->g.vh;
   CUDA_OR_FAIL(h, cudaMemcpyAsync(host_out, h->rng, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
   unsigned long long* c = reinterpret_cast<unsigned long long*>(&h->result_host[3]);
@@ -1070,6 +1090,8 @@ int qcd_store_rng(qcd_lattice* h, uint32_t* host_out) {
 
 int qcd_load_rng(qcd_lattice* h, const uint32_t* host_in) {
   if (!h || !host_in) return QCD_ERR_INVALID;
+  int rc0 = ensure_rng(h);
+  if (rc0) return rc0;
   const size_t n = 6 * (size_t)h->g.vh;
   const unsigned long long c = (unsigned long long)host_in[n] | ((unsigned long long)host_in[n + 1] << 32);
   CUDA_OR_FAIL(h, cudaMemcpyAsync(h->rng, host_in, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));

@@ -1,0 +1,138 @@
+"""Per-link checks of the FP32 kernels against the oracle's FP32 restatement.
+
+The FP32 heat-bath, Metropolis and over-relaxation kernels produce the
+benchmark's numbers.  Here one pass of each, from the same configuration and
+the same Philox counters, is compared link by link with the CPU restatement
+(oracle.c, ora_phase32), on all three boundary conditions and on ragged and
+tiny lattices.  Both sides compute in float with the same operation order;
+they differ by rounding (nvcc's multiply-add contraction, rsqrtf, and the
+GPU's hardware cos/log/sincos in the heat-bath against host libm), so:
+
+* over-relaxation (deterministic) must agree to OR_TOL on every link;
+* heat-bath and Metropolis must agree to DRAW_TOL on every link except where
+  a rounding difference moved a rejection-loop or accept decision; such
+  sites are counted, and together with the links whose staples they feed in
+  the later phases of the pass they must stay below MAX_FLIPPED.
+
+Reference algorithm: functions/mc_updates.h:7-64,109-115 (heat-bath,
+Metropolis, over-relaxation) with the PCC/PMC masks of mc_updates_pcc.h and
+mc_updates_pmc.h:33,40.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+import qcd_2d_gpu_b200 as q
+
+pytestmark = pytest.mark.gpu
+
+OR_TOL = 2e-5    # one pass of 6 phases, float rounding only
+DRAW_TOL = 2e-5  # same, for the links whose draws led to the same decisions
+FLIP_TOL = 1e-3  # a link further off than this took another branch somewhere
+# A moved decision changes one link by O(1), and the staples of the links
+# updated after it in the same pass: a few dozen links at most.  With the
+# rounding above a decision moves with probability ~1e-7 per update, so this
+# bound is almost never approached.
+MAX_FLIPPED = 64
+
+CASES = [((8, 6, 10), 0), ((8, 6, 10), 1), ((8, 6, 10), 2), ((16, 16, 16), 2), ((2, 2, 2), 0), ((4, 2, 6), 1),
+         ((32, 8, 16), 2)]
+
+
+def counter_and_key(L):
+    w = L.store_rng()
+    return int(w[-4]) | (int(w[-3]) << 32), int(w[-2]) | (int(w[-1]) << 32)
+
+
+def thermalised(dims, bc, beta, algo="hb", seed=7, **kw):
+    L = q.Lattice(*dims, beta, algo=algo, boundary=bc, precision="fp32", seed=seed, **kw)
+    L.init_hot()
+    L.sweep(4)
+    return L
+
+
+def link_dev(a, b):
+    return np.abs(a.reshape(-1, 4) - b.reshape(-1, 4)).max(axis=1)
+
+
+@pytest.mark.parametrize("dims,bc", CASES)
+def test_fp32_overrelaxation_pass_matches_oracle(dims, bc):
+    L = thermalised(dims, bc, 7.0)
+    cfg = L.store_config()
+    o = po.Oracle(*dims, 7.0, algo=1, boundary=bc)
+    o.load(cfg)
+    L.overrelax(1)
+    for k in range(6):
+        o.phase32(k, 2)
+    d = link_dev(L.store_config(), o.field())
+    L.close()
+    o.close()
+    assert d.max() <= OR_TOL, d.max()
+
+
+@pytest.mark.parametrize("dims,bc", CASES)
+@pytest.mark.parametrize("renorm", [False, True])
+def test_fp32_heatbath_pass_matches_oracle(dims, bc, renorm):
+    beta = 9.0
+    L = thermalised(dims, bc, beta, renorm_every=1 if renorm else 0)
+    cfg = L.store_config()
+    ctr, key = counter_and_key(L)
+    o = po.Oracle(*dims, beta, algo=1, boundary=bc)
+    o.load(cfg)
+    L.sweep(1)  # one heat-bath pass (re-projected as it is stored when renorm)
+    tries = np.zeros(L.V, np.int32)
+    for k in range(6):
+        o.phase32(k, 1, key, ctr + k, renorm, hb_tries=tries)
+    d = link_dev(L.store_config(), o.field())
+    L.close()
+    o.close()
+    flipped = int((d > FLIP_TOL).sum())
+    assert flipped <= MAX_FLIPPED, (flipped, d.max())
+    assert np.sort(d)[len(d) - flipped - 1] <= DRAW_TOL
+    assert tries.max() >= 1
+
+
+@pytest.mark.parametrize("dims,bc", CASES[:4])
+def test_fp32_metropolis_pass_matches_oracle(dims, bc):
+    beta, eps, upd = 6.0, 0.3, 3
+    L = thermalised(dims, bc, beta, algo="metro", epsilon=eps, upd=upd)
+    cfg = L.store_config()
+    ctr, key = counter_and_key(L)
+    L.accept_reset()
+    o = po.Oracle(*dims, beta, algo=0, boundary=bc, epsilon=eps, upd=upd)
+    o.load(cfg)
+    L.sweep(1)
+    for k in range(6):
+        o.phase32(k, 0, key, ctr + k)
+    d = link_dev(L.store_config(), o.field())
+    acc_gpu, acc_ora = L.accept_counts(), o.accept()
+    L.close()
+    o.close()
+    flipped = int((d > FLIP_TOL).sum())
+    assert flipped <= MAX_FLIPPED, (flipped, d.max())
+    assert np.sort(d)[len(d) - flipped - 1] <= DRAW_TOL
+    # accept decisions: identical except at the few sites a rounding difference moved
+    assert int((acc_gpu != acc_ora).sum()) <= 4
+    assert acc_gpu.sum() > 0
+
+
+def test_fp32_sweep_with_overrelaxation_and_renorm_matches_oracle():
+    # the headline sweep's shape on a small PMC lattice: a heat-bath pass, then
+    # an over-relaxation pass that re-projects each link as it stores it
+    dims, bc, beta = (12, 10, 14), 2, 10.0
+    L = thermalised(dims, bc, beta, n_or=1, renorm_every=1)
+    cfg = L.store_config()
+    ctr, key = counter_and_key(L)
+    o = po.Oracle(*dims, beta, algo=1, boundary=bc)
+    o.load(cfg)
+    L.sweep(1)
+    for k in range(6):
+        o.phase32(k, 1, key, ctr + k)
+    for k in range(6):
+        o.phase32(k, 2, renorm=True)
+    d = link_dev(L.store_config(), o.field())
+    L.close()
+    o.close()
+    flipped = int((d > FLIP_TOL).sum())
+    assert flipped <= 2 * MAX_FLIPPED, (flipped, d.max())
+    assert np.sort(d)[len(d) - flipped - 1] <= 5 * DRAW_TOL

@@ -59,3 +59,22 @@ def test_site_and_phase_counters_give_uniform_words():
     h, _ = np.histogram(u, bins=16, range=(0, 1))
     chi2 = ((h - 256.0) ** 2 / 256.0).sum()
     assert chi2 < 40  # 15 degrees of freedom: p ~ 5e-4
+
+
+@pytest.mark.parametrize("ctr,key,out", KAT)
+def test_oracle_restatement_matches_the_known_answers(ctr, key, out):
+    # the CPU oracle's own Philox (the checker of the FP32 kernels) is pinned
+    # to the same published vectors
+    import pyoracle as po
+
+    assert tuple(int(v) for v in po.philox4x32(ctr, key)) == out
+
+
+def test_oracle_restatement_matches_the_library_on_many_counters():
+    import pyoracle as po
+
+    rng = np.random.default_rng(5)
+    for _ in range(200):
+        c = rng.integers(0, 2 ** 32, 4, dtype=np.uint64).astype(np.uint32)
+        k = rng.integers(0, 2 ** 32, 2, dtype=np.uint64).astype(np.uint32)
+        assert np.array_equal(po.philox4x32(c, k), q.philox4x32(c, k))
