@@ -415,7 +415,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-replica measurement")
     ap.add_argument("--lattice", type=int, nargs=3, default=None, help="override (testing only)")
     ap.add_argument("--workload", default="sweep", choices=["sweep", "accuracy", "c3-accuracy"])
-    ap.add_argument("--schedule", default="auto", choices=["auto", "phases", "wavefront"])
+    ap.add_argument("--schedule", default="auto", choices=["auto", "phases", "wavefront", "pairs"])
     ap.add_argument("--wave-tuning", type=int, nargs=3, default=None, metavar=("CHUNK", "PASSES", "FRONTS"))
     ap.add_argument("--scan-size", type=int, default=128)
     ap.add_argument("--scan-sweeps", type=int, default=2000)

@@ -158,12 +158,24 @@ int qcd_check_unitarity(qcd_lattice* h, double tol, double* mean_det);
  *              tasks run in a ring schedule ordered so that each waits only
  *              for earlier ones (bounded waits, QCD_ERR_TIMEOUT otherwise).
  *              Bit-identical to PHASES.
+ *   PAIRS      FP32 only: each pass as three launches, one per direction mu,
+ *              each fusing the phases (mu, even) and (mu, odd).  A CTA owns a
+ *              tile of the plane perpendicular to its streamed direction and
+ *              walks along it with the six link classes of the coming slices
+ *              staged in shared memory by bulk asynchronous copies, so a link
+ *              leaves HBM about once per pair instead of once per phase.  The
+ *              pass writes its links into a second store (allocated when the
+ *              schedule is set) that then becomes current.  Same updates and
+ *              draws as PHASES; results agree with it to float rounding.
  *   AUTO       the schedule measured fastest for the lattice (currently PHASES).
  * ------------------------------------------------------------------------ */
-enum qcd_schedule { QCD_SCHED_AUTO = 0, QCD_SCHED_PHASES = 1, QCD_SCHED_WAVEFRONT = 2 };
+enum qcd_schedule { QCD_SCHED_AUTO = 0, QCD_SCHED_PHASES = 1, QCD_SCHED_WAVEFRONT = 2, QCD_SCHED_PAIRS = 3 };
 int qcd_set_schedule(qcd_lattice* h, int mode);
-/* the schedule qcd_sweep will use (PHASES or WAVEFRONT) */
+/* the schedule qcd_sweep will use (PHASES, WAVEFRONT or PAIRS) */
 int qcd_get_schedule(const qcd_lattice* h);
+/* Fused pairs: streamed slices per CTA (0: automatic, enough CTAs for every
+   SM several times over). */
+int qcd_set_pair_tuning(qcd_lattice* h, int slices_per_cta);
 /* Wavefront knobs (0 keeps the current value): sites per task (rounded up to
    a multiple of 256), passes chained per launch (1..4; more passes keep more
    slices live in L2) and fronts (a divisor of Lt leaving arcs of >= 2 slices:
@@ -179,8 +191,9 @@ int qcd_set_wave_tuning(qcd_lattice* h, int chunk_sites, int passes_per_launch, 
    precision, algorithm, boundary, n_or) for the life of the process, so later
    handles of the same shape reuse it without timing. */
 typedef struct qcd_tuning {
-  int schedule;           /* QCD_SCHED_PHASES or QCD_SCHED_WAVEFRONT */
-  int chunk_sites, passes_per_launch, fronts;
+  int schedule;           /* QCD_SCHED_PHASES, QCD_SCHED_WAVEFRONT or QCD_SCHED_PAIRS */
+  int chunk_sites;        /* wavefront: sites per task; pairs: streamed slices per CTA (0 automatic) */
+  int passes_per_launch, fronts;
   double ms_per_sweep;    /* measured time of the chosen candidate */
 } qcd_tuning;
 int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen);

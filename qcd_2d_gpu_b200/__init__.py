@@ -31,7 +31,8 @@ LIB_PATH = os.path.join(_HERE, "libqcd2d.so")
 METROPOLIS, HEATBATH = 0, 1
 PERIODIC, PCC, PMC = 0, 1, 2
 FP64, FP32 = 0, 1
-SCHED_AUTO, SCHED_PHASES, SCHED_WAVEFRONT = 0, 1, 2
+SCHED_AUTO, SCHED_PHASES, SCHED_WAVEFRONT, SCHED_PAIRS = 0, 1, 2, 3
+_SCHED_NAME = {SCHED_PHASES: "phases", SCHED_WAVEFRONT: "wavefront", SCHED_PAIRS: "pairs"}
 
 _BC = {"periodic": PERIODIC, "per": PERIODIC, "pcc": PCC, "pmc": PMC}
 _ALGO = {"metropolis": METROPOLIS, "metro": METROPOLIS, "heatbath": HEATBATH, "hb": HEATBATH}
@@ -156,6 +157,7 @@ _SIGS = {
     "qcd_wave_plan": (_I, [_P, _P, _I, _P, _P, _P]),
     "qcd_wave_selftest_timeout": (_I, [_P]),
     "qcd_set_wave_tuning": (_I, [_P, _I, _I, _I]),
+    "qcd_set_pair_tuning": (_I, [_P, _I]),
     "qcd_rng_words": (ctypes.c_longlong, [_P]),
     "qcd_philox4x32": (None, [_P, _P, _P]),
     "qcd_store_rng": (_I, [_P, _P]),
@@ -280,21 +282,24 @@ class Lattice:
         self._check(self._lib.qcd_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)), "set_stream")
 
     def set_schedule(self, mode: int | str) -> None:
-        m = {"auto": SCHED_AUTO, "phases": SCHED_PHASES, "wavefront": SCHED_WAVEFRONT}.get(mode, mode)
+        m = {"auto": SCHED_AUTO, "phases": SCHED_PHASES, "wavefront": SCHED_WAVEFRONT, "pairs": SCHED_PAIRS}.get(mode, mode)
         self._check(self._lib.qcd_set_schedule(self._h, int(m)), "set_schedule")
 
     def schedule(self) -> str:
-        return {SCHED_PHASES: "phases", SCHED_WAVEFRONT: "wavefront"}[self._lib.qcd_get_schedule(self._h)]
+        return _SCHED_NAME[self._lib.qcd_get_schedule(self._h)]
 
     def set_wave_tuning(self, chunk_sites: int = 0, passes_per_launch: int = 0, fronts: int = 0) -> None:
         self._check(self._lib.qcd_set_wave_tuning(self._h, chunk_sites, passes_per_launch, fronts),
                     "set_wave_tuning")
 
+    def set_pair_tuning(self, slices_per_cta: int = 0) -> None:
+        self._check(self._lib.qcd_set_pair_tuning(self._h, slices_per_cta), "set_pair_tuning")
+
     def autotune(self, sweeps_per_trial: int = 0) -> dict:
         """Pick the fastest schedule for this lattice (state is preserved)."""
         t = Tuning()
         self._check(self._lib.qcd_autotune(self._h, sweeps_per_trial, ctypes.byref(t)), "autotune")
-        return {"schedule": {SCHED_PHASES: "phases", SCHED_WAVEFRONT: "wavefront"}[t.schedule],
+        return {"schedule": _SCHED_NAME[t.schedule],
                 "chunk_sites": t.chunk_sites, "passes_per_launch": t.passes_per_launch, "fronts": t.fronts,
                 "ms_per_sweep": t.ms_per_sweep}
 

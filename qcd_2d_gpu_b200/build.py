@@ -39,22 +39,38 @@ def needs_build() -> bool:
     return any(os.path.getmtime(s) > t for s in deps)
 
 
+UNITS = ["qcd2d.cu", "batch.cu", "pairs.cu", "stats.cc"]
+
+
 def build_library(force: bool = False, verbose: bool = False) -> str:
+    """Compile every translation unit for sm_100a in parallel, then link the
+    shared library (nvcc -shared)."""
     if not force and not needs_build():
         return LIB
+    import concurrent.futures as cf
+    import tempfile
+
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + [
-        "-I" + os.path.join(ROOT, "include"),
-        "-I" + CSRC,
-        "-o",
-        LIB + ".tmp",
-        os.path.join(CSRC, "qcd2d.cu"),
-        os.path.join(CSRC, "batch.cu"),
-        os.path.join(CSRC, "stats.cc"),
-    ]
-    if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True)
+    inc = ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    with tempfile.TemporaryDirectory(prefix="qcd2d_build_") as tmp:
+        objs, cmds = [], []
+        for u in UNITS:
+            obj = os.path.join(tmp, u + ".o")
+            objs.append(obj)
+            cmds.append([nvcc] + compile_flags + inc + ["-c", os.path.join(CSRC, u), "-o", obj])
+        with cf.ThreadPoolExecutor(max_workers=len(cmds)) as ex:
+            futs = []
+            for c in cmds:
+                if verbose:
+                    print(" ".join(c), flush=True)
+                futs.append(ex.submit(subprocess.run, c, check=True))
+            for f in futs:
+                f.result()
+        link = [nvcc] + NVCC_FLAGS + ["-o", LIB + ".tmp"] + objs
+        if verbose:
+            print(" ".join(link), flush=True)
+        subprocess.run(link, check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -1,0 +1,343 @@
+// Fused even/odd pairs of the FP32 sweep, streamed through shared memory by
+// bulk asynchronous copies (the TMA engine), for B200 (sm_100a).
+//
+// The six phases of a pass come in pairs (MU, even), (MU, odd).  Within a
+// pair, U_MU couples only to sites displaced perpendicular to MU, so a pair
+// can be run as a stream: one CTA owns a tile of rows x y' and walks along a
+// streamed direction S (t for MU = y, x; x for MU = t).  At step j it updates
+// the even U_MU of slice e and the odd U_MU of slice e - 2; the odd update
+// needs the new even links of slices e-3 .. e-1, all made at earlier steps, so
+// the two halves of a step are independent and one block barrier per step
+// suffices.  The third direction R (y for MU = x, t; x for MU = y) has no
+// streaming order: the even links of a one-site ring around the tile are
+// recomputed by each CTA that needs them (their inputs are old links, so the
+// recomputation is exact).
+//
+// Data flow per CTA (one per SM; 226 KB of shared memory):
+//   * seven planes of NS x NR x W float4: the six link classes (direction,
+//     parity) of NS consecutive slices of the tile and its halo, filled row by
+//     row with cp.async.bulk from HBM/L2, and the new even U_MU of the same
+//     slices;
+//   * NS mbarriers, one per slice slot; a slot is refilled with the slice NS
+//     ahead once the block barrier shows nobody reads it, so every load is
+//     issued two steps before it is needed;
+//   * results go straight from registers to the other copy of the link store:
+//     the pair reads the current store and writes U_MU into the second one,
+//     so a CTA recomputing a ring never sees a neighbour's new links.
+//
+// Every link update is the one of the per-phase kernels (link_update32, same
+// draws: the Philox counter is the site's global sublattice index and the
+// phase number), the staples now gathered from shared memory.
+//
+// Bulk copies need 16-byte aligned addresses and sizes: links are float4 and
+// the stores come from cudaMalloc.  No copy uses cluster multicast.
+#pragma once
+#include <stdint.h>
+#include "sites.cuh"
+
+namespace qcd {
+
+constexpr int kPairNS = 7;      // slice slots
+constexpr int kPairNR = 17;     // staged rows
+constexpr int kPairW = 17;      // staged y' window
+constexpr int kPairPlanes = 7;  // six link classes + the new even links of MU
+constexpr int kPairPlane = kPairNS * kPairNR * kPairW;  // float4 per plane
+constexpr int kPairSlotStride = kPairNR * kPairW;       // float4 per slot of a plane
+constexpr size_t kPairSmemBytes = (size_t)kPairPlanes * kPairPlane * sizeof(float4) + kPairNS * sizeof(uint64_t);
+constexpr unsigned int kPairFillBytes = 6u * kPairNR * kPairW * sizeof(float4);  // one slice of six classes
+constexpr unsigned long long kPairWaitNs = 200000000ull;  // bound of one wait: 0.2 s, far above any real load
+
+// Frame of the pair kernel for direction MU.
+//   S      streamed direction
+//   ROW    direction of the staged rows (the other one of x, t)
+//   TR     tile rows;  ROW0: staged row of the first tile row
+//   TY     tile y' per row;  W0: window column of the first tile y'
+//   YRING  the ring is in y (MU = x, t) or in the rows (MU = y)
+//   NT     threads: one per site update of a step
+template <int MU>
+struct PairCfg;
+template <>
+struct PairCfg<DIR_X> {
+  static constexpr int S = DIR_T, ROW = DIR_X, TR = 16, ROW0 = 0, TY = 15, W0 = 1, NT = 512;
+  static constexpr bool YRING = true;
+};
+template <>
+struct PairCfg<DIR_T> {
+  static constexpr int S = DIR_X, ROW = DIR_T, TR = 16, ROW0 = 0, TY = 15, W0 = 1, NT = 512;
+  static constexpr bool YRING = true;
+};
+template <>
+struct PairCfg<DIR_Y> {
+  static constexpr int S = DIR_T, ROW = DIR_X, TR = 13, ROW0 = 2, TY = 16, W0 = 0, NT = 448;
+  static constexpr bool YRING = false;
+};
+// even items (tile + ring) and odd items (tile) of a full tile fit one per thread
+static_assert(16 * 16 + 16 * 15 <= 512, "x/t pair items");
+static_assert(15 * 16 + 13 * 16 <= 448, "y pair items");
+// staged rows and window cover the stencil: +1 row (MU = x, t) or ring +-1 and
+// stencil +-1 rows (MU = y); ring +-1 and stencil +-1 in y' (MU = x, t) or +y (MU = y)
+static_assert(16 + 1 <= kPairNR && 13 + 4 <= kPairNR, "rows");
+static_assert(15 + 2 <= kPairW && 16 + 1 <= kPairW, "window");
+
+struct PairPlanes {
+  const float4* src[6];  // the current link classes, plane d*2 + p
+  float4* dst_e;         // U_MU(even) of the other store
+  float4* dst_o;         // U_MU(odd) of the other store
+};
+
+struct PairGrid {
+  int n_row_tiles;  // tiles along ROW
+  int seg;          // streamed slices per CTA
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ int pmod(int a, int n) {
+  a %= n;
+  return a < 0 ? a + n : a;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned int bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool mbar_test(uint32_t addr, unsigned int parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(addr), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Bounded wait for the completion of the phase with the given parity: false
+// after kPairWaitNs of wall time, or as soon as any CTA has flagged a timeout
+// in the device error word (so one stuck load ends the whole launch quickly).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned int parity, const int* err) {
+  const uint32_t addr = smem_u32(bar);
+  unsigned long long t0 = 0;
+  for (unsigned int i = 0;; i++) {
+    if (mbar_test(addr, parity)) return true;
+    if ((i & 63) == 63) {
+      if (*(const volatile int*)err & DEVERR_TIMEOUT) return false;
+      const unsigned long long t = global_ns();
+      if (t0 == 0)
+        t0 = t;
+      else if (t - t0 > kPairWaitNs)
+        return false;
+    }
+  }
+}
+// Bounded wait for this CTA's own copies before it exits after a timeout.
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, unsigned int parity) {
+  const uint32_t addr = smem_u32(bar);
+  const unsigned long long t0 = global_ns();
+  while (!mbar_test(addr, parity) && global_ns() - t0 < kPairWaitNs) {
+  }
+}
+// bytes (a multiple of 16) from global src to shared dst, completing on bar
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned int bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// The links of a step as the staple gather sees them: plane d*2 + p of the
+// staged slices; in the odd half, U_MU(even) comes from the new-link plane.
+template <int MU, bool ODD>
+struct PairSmem {
+  const float4* base;
+  __device__ __forceinline__ Quat<float> ld(int dir, int par, int idx) const {
+    const int plane = (ODD && dir == MU && par == 0) ? 6 : dir * 2 + par;
+    const float4 v = base[plane * kPairPlane + idx];
+    return Quat<float>{v.x, v.y, v.z, v.w};
+  }
+  __device__ __forceinline__ Quat<float> ld_own(int dir, int par, int idx) const { return ld(dir, par, idx); }
+};
+
+// Fill slot `slot` with unwrapped slice sx of the tile's rows and window:
+// 6 classes x NR rows, each row one or (where the window wraps) more bulk
+// copies.  Called by all 32 lanes of one warp.
+template <int MU>
+__device__ __forceinline__ void pair_fill(float4* sm, uint64_t* bar, int slot, int sx, const PairPlanes& P,
+                                          const Geo& g, int R0, int Y0h, int lane) {
+  typedef PairCfg<MU> C;
+  const int ls = C::S == DIR_T ? g.lt : g.lx, lrow = C::ROW == DIR_T ? g.lt : g.lx;
+  const int s = pmod(sx, ls);
+  if (lane == 0) {
+    // the generic-proxy reads of this slot (before the block barrier) come
+    // before the asynchronous writes that refill it
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(bar, kPairFillBytes);
+  }
+  __syncwarp();
+  if (lane < kPairNR) {
+    const int r = lane;
+    const int gr = pmod(R0 - C::ROW0 + r, lrow);
+    const int t = C::S == DIR_T ? s : gr, x = C::S == DIR_T ? gr : s;
+    const size_t row_off = (size_t)g.lyh * (size_t)(x + g.lx * t);
+    const int y0 = pmod(Y0h - C::W0, g.lyh);
+#pragma unroll
+    for (int p = 0; p < 6; p++) {
+      const float4* src = P.src[p] + row_off;
+      float4* dst = sm + p * kPairPlane + slot * kPairSlotStride + r * kPairW;
+      int w = 0, y = y0;
+      while (w < kPairW) {
+        const int n = min(kPairW - w, g.lyh - y);
+        bulk_load(dst + w, src + y, (unsigned int)n * 16u, bar);
+        w += n;
+        y = 0;
+      }
+    }
+  }
+}
+
+// One fused pair (MU, even) + (MU, odd) over one segment of the streamed
+// direction for one tile.  Grid: (row tiles x y tiles, segments).
+template <int MU, int BC, int KIND>
+__global__ void __launch_bounds__(PairCfg<MU>::NT, 1)
+    pair32(PairPlanes P, Geo g, PhaseArgs a, PairGrid pg) {
+  typedef PairCfg<MU> C;
+  extern __shared__ __align__(128) float4 sm[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kPairPlanes * kPairPlane);
+  __shared__ int abort_flag;
+
+  const int ls = C::S == DIR_T ? g.lt : g.lx, lrow = C::ROW == DIR_T ? g.lt : g.lx;
+  const int rt = blockIdx.x % pg.n_row_tiles, yt = blockIdx.x / pg.n_row_tiles;
+  const int R0 = rt * C::TR, Y0h = yt * C::TY;
+  const int nr = min(C::TR, lrow - R0), ny = min(C::TY, g.lyh - Y0h);
+  const int s0 = blockIdx.y * pg.seg, s1 = min(s0 + pg.seg, ls);
+  const int first = s0 - 2, last = s1 + 1;  // unwrapped slices staged
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (tid == 0) {
+    abort_flag = 0;
+    for (int i = 0; i < kPairNS; i++) mbar_init(&bars[i], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (warp == 0)
+    for (int x = first; x <= last && x < first + kPairNS; x++)
+      pair_fill<MU>(sm, &bars[x - first], x - first, x, P, g, R0, Y0h, lane);
+
+  // this thread's item: an even site (tile + ring) or an odd site (tile)
+  const int ne_row = C::YRING ? ny + 1 : ny;                  // even items per row
+  const int ne_rows = C::YRING ? nr : nr + 2;                 // even rows
+  const int n_even = ne_row * ne_rows, n_odd = ny * nr;
+  const bool is_even = tid < n_even, is_odd = !is_even && tid < n_even + n_odd;
+  int r = 0, i = 0;
+  if (is_even) {
+    r = tid / ne_row;
+    i = tid - r * ne_row;
+    r += C::YRING ? C::ROW0 : C::ROW0 - 1;
+  } else if (is_odd) {
+    const int u = tid - n_even;
+    r = u / ny;
+    i = u - r * ny;
+    r += C::ROW0;
+  }
+  const int grow = pmod(R0 - C::ROW0 + r, lrow);  // global row coordinate
+  const bool tile_row = r >= C::ROW0 && r < C::ROW0 + nr;
+  int issued = min(last, first + kPairNS - 1);  // last slice whose fill was issued
+
+  const int J = s1 - s0 + 3;
+  for (int j = 0; j < J; j++) {
+    const int e = s0 - 1 + j, o = e - 2;
+    // wait for the slices first read at this step
+    bool ok = true;
+    if (j == 0) {
+      for (int x = first; x <= e && ok; x++) ok = mbar_wait(&bars[(x - first) % kPairNS], ((x - first) / kPairNS) & 1, a.err);
+    }
+    if (ok && e + 1 <= last) ok = mbar_wait(&bars[(e + 1 - first) % kPairNS], ((e + 1 - first) / kPairNS) & 1, a.err);
+    if (!ok) {
+      atomicOr(a.err, DEVERR_TIMEOUT);
+      abort_flag = 1;
+    }
+    if (ok && (is_even || is_odd)) {
+      // slice of this thread's update and its slot
+      const int sx = is_even ? e : o;
+      const bool active = is_even ? (e <= s1) : (o >= s0);
+      if (active) {
+        const int slot = (sx - first) % kPairNS;
+        const int gs = pmod(sx, ls);
+        const int par = is_even ? 0 : 1;
+        // parity of the physical y of sublattice `par` on this row of slice sx
+        const int q = ((sx + grow) & 1) ^ par;
+        // window column: even items of a y-ring row start one column early
+        // when their physical y is odd
+        const int w = C::YRING ? (is_even ? C::W0 - q + i : C::W0 + i) : i;
+        const int yq = pmod(Y0h - C::W0 + w, g.lyh);
+        const int t = C::S == DIR_T ? gs : grow, xg = C::S == DIR_T ? grow : gs;
+        const int gid = yq + g.lyh * (xg + g.lx * t);
+        Nbr n;
+        n.id = slot * kPairSlotStride + r * kPairW + w;
+        n.yq = yq;
+        n.q = q;
+        n.x = xg;
+        n.t = t;
+        n.yp = q ? 1 : 0;
+        n.ym = q ? 0 : -1;
+        const int sp = slot == kPairNS - 1 ? -(kPairNS - 1) * kPairSlotStride : kPairSlotStride;
+        const int sm_ = slot == 0 ? (kPairNS - 1) * kPairSlotStride : -kPairSlotStride;
+        if (C::ROW == DIR_X) {
+          n.xp = kPairW;
+          n.xm = -kPairW;
+          n.tp = sp;
+          n.tm = sm_;
+        } else {
+          n.tp = kPairW;
+          n.tm = -kPairW;
+          n.xp = sp;
+          n.xm = sm_;
+        }
+        const bool in_tile = C::YRING ? (w >= C::W0 && w < C::W0 + ny) : tile_row;
+        const bool in_seg = sx >= s0 && sx < s1;
+        PhaseArgs ap = a;
+        ap.phase_off = a.phase_off + (unsigned int)par;
+        Quat<float> U;
+        if (is_even) {
+          const PairSmem<MU, false> L{sm};
+          if (BC == BC_PCC && MU != DIR_Y && at_y0(g, n))
+            U = L.ld_own(MU, 0, n.id);  // frozen: the old link carries over
+          else
+            U = link_update32<MU, 0, BC, KIND>(L, g, ap, n, gid, a.renorm, in_tile && in_seg);
+          sm[6 * kPairPlane + n.id] = make_float4(U.w, U.x, U.y, U.z);
+          if (in_tile && in_seg) P.dst_e[gid] = make_float4(U.w, U.x, U.y, U.z);
+        } else {
+          const PairSmem<MU, true> L{sm};
+          if (BC == BC_PCC && MU != DIR_Y && at_y0(g, n))
+            U = L.ld_own(MU, 1, n.id);
+          else
+            U = link_update32<MU, 1, BC, KIND>(L, g, ap, n, gid, a.renorm, true);
+          P.dst_o[gid] = make_float4(U.w, U.x, U.y, U.z);
+        }
+      }
+    }
+    __syncthreads();
+    if (abort_flag) break;
+    // the slot of slice e - 3 is free: refill it with slice e - 3 + NS
+    const int fx = e - 3 + kPairNS;
+    if (e - 3 >= first && fx <= last) {
+      if (warp == 0) pair_fill<MU>(sm, &bars[(fx - first) % kPairNS], (fx - first) % kPairNS, fx, P, g, R0, Y0h, lane);
+      issued = fx;
+    }
+  }
+  if (abort_flag && tid == 0) {
+    // leave no copy in flight into this CTA's shared memory: wait (bounded)
+    // for the latest fill of every slot
+    for (int x = max(first, issued - kPairNS + 1); x <= issued; x++)
+      mbar_drain(&bars[(x - first) % kPairNS], ((x - first) / kPairNS) & 1);
+  }
+}
+
+}  // namespace qcd

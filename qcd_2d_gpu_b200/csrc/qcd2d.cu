@@ -13,6 +13,7 @@
 #include <new>
 #include <vector>
 #include "kernels.cuh"
+#include "pairs.h"
 #include "qcd2d.h"
 #include "wave.cuh"
 
@@ -27,7 +28,8 @@ struct qcd_lattice {
   // link store
   double2* lo = nullptr;
   double2* hi = nullptr;
-  float4* q32 = nullptr;
+  float4* q32 = nullptr;     // FP32 store holding the current links
+  float4* q32alt = nullptr;  // second FP32 store: the fused-pair schedule writes each pass's new links here
   size_t link_bytes = 0;
   // MRG32k3a streams, 6 u32 planes
   uint32_t* rng = nullptr;
@@ -63,6 +65,8 @@ struct qcd_lattice {
   unsigned int* wave_tasks[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // per chain length
   int wave_tasks_chunk[5] = {0, 0, 0, 0, 0};
   int wave_tasks_fronts[5] = {0, 0, 0, 0, 0};
+  int sms = 0;       // multiprocessors of the device (fused pairs)
+  int pair_seg = 0;  // fused pairs: streamed slices per CTA (0: automatic)
   char msg[512] = {0};
 };
 
@@ -445,6 +449,38 @@ bool use_wave(const qcd_lattice* h) {
   return h->sched == QCD_SCHED_WAVEFRONT;
 }
 
+bool use_pairs(const qcd_lattice* h) { return h->sched == QCD_SCHED_PAIRS && h->p.precision == QCD_PREC_FP32; }
+
+// The second store and the device facts the fused pairs need (allocated
+// when the schedule is chosen, never inside a pass, so that passes can be
+// captured in a CUDA graph).
+int pairs_setup(qcd_lattice* h) {
+  if (!h->q32alt) CUDA_OR_FAIL(h, cudaMalloc(&h->q32alt, h->link_bytes));
+  if (!h->sms) {
+    int dev = 0;
+    CUDA_OR_FAIL(h, cudaGetDevice(&dev));
+    CUDA_OR_FAIL(h, cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  return QCD_OK;
+}
+
+// One pass as three fused pairs (y, x, t), reading the current store and
+// writing the other one, which then becomes current.
+int pass_pairs(qcd_lattice* h, int kind, int renorm) {
+  if (!h->q32alt || !h->sms) return fail(h, QCD_ERR_INVALID, "fused pairs used before their setup");
+  PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, renorm, h->draw_key, h->draw_dev, 0, 0};
+  CUDA_OR_FAIL(h, pair_pass32(h->q32, h->q32alt, h->g, h->p.boundary, kind, a, h->pair_seg, h->sms, h->stream));
+  float4* t = h->q32;
+  h->q32 = h->q32alt;
+  h->q32alt = t;
+  if (kind != KIND_METRO) h->unit_passes++;
+  if (kind != KIND_OR) {
+    advance_counter<<<1, 1, 0, h->stream>>>(h->draw_dev, 6ull);
+    LAUNCH_CHECK(h);
+  }
+  return QCD_OK;
+}
+
 int run_passes(qcd_lattice* h, const PassSpec* ps, int np);
 
 int check_device_error(qcd_lattice* h) {
@@ -456,7 +492,8 @@ int check_device_error(qcd_lattice* h) {
   if (e & DEVERR_TIMEOUT) {
     CUDA_OR_FAIL(h, cudaMemsetAsync(h->err, 0, sizeof(int), h->stream));
     CUDA_OR_FAIL(h, cudaStreamSynchronize(h->stream));
-    return fail(h, QCD_ERR_TIMEOUT, "a wavefront task waited longer than its bound for a neighbour slice");
+    return fail(h, QCD_ERR_TIMEOUT, "a bounded device wait ran out (a wavefront task waiting for a neighbour slice, "
+                                     "or a fused-pair CTA waiting for its staged links)");
   }
   if (e & DEVERR_HB_LOOP)
     return fail(h, QCD_ERR_NONUNITARY,
@@ -495,6 +532,13 @@ int launch_measure(qcd_lattice* h, double* out_dev) {
 
 int run_passes(qcd_lattice* h, const PassSpec* ps, int np) {
   if (np == 0) return QCD_OK;
+  if (use_pairs(h)) {
+    for (int i = 0; i < np; i++) {
+      int rc = pass_pairs(h, ps[i].kind, ps[i].renorm);
+      if (rc) return rc;
+    }
+    return QCD_OK;
+  }
   if (use_wave(h)) {
     int rc = wave_setup(h);
     if (rc) return rc;
@@ -528,6 +572,7 @@ void release(qcd_lattice* h) {
   cudaFree(h->lo);
   cudaFree(h->hi);
   cudaFree(h->q32);
+  cudaFree(h->q32alt);
   cudaFree(h->rng);
   cudaFree(h->accept);
   cudaFree(h->partials);
@@ -797,14 +842,26 @@ int qcd_overrelax(qcd_lattice* h, int n) {
 }
 
 int qcd_set_schedule(qcd_lattice* h, int mode) {
-  if (!h || mode < QCD_SCHED_AUTO || mode > QCD_SCHED_WAVEFRONT) return QCD_ERR_INVALID;
+  if (!h || mode < QCD_SCHED_AUTO || mode > QCD_SCHED_PAIRS) return QCD_ERR_INVALID;
+  if (mode == QCD_SCHED_PAIRS) {
+    if (h->p.precision != QCD_PREC_FP32)
+      return fail(h, QCD_ERR_UNSUPPORTED, "fused pairs are an FP32 schedule (FP64 keeps the reference's kernels)");
+    int rc = pairs_setup(h);
+    if (rc) return rc;
+  }
   h->sched = mode;
   return QCD_OK;
 }
 
 int qcd_get_schedule(const qcd_lattice* h) {
   if (!h) return QCD_ERR_INVALID;
-  return use_wave(h) ? QCD_SCHED_WAVEFRONT : QCD_SCHED_PHASES;
+  return use_pairs(h) ? QCD_SCHED_PAIRS : use_wave(h) ? QCD_SCHED_WAVEFRONT : QCD_SCHED_PHASES;
+}
+
+int qcd_set_pair_tuning(qcd_lattice* h, int slices_per_cta) {
+  if (!h || slices_per_cta < 0) return QCD_ERR_INVALID;
+  h->pair_seg = slices_per_cta;
+  return QCD_OK;
 }
 
 int qcd_set_wave_tuning(qcd_lattice* h, int chunk_sites, int passes_per_launch, int fronts) {
@@ -840,6 +897,7 @@ int apply_tuning(qcd_lattice* h, const qcd_tuning& t) {
   int rc = qcd_set_schedule(h, t.schedule);
   if (rc == QCD_OK && t.schedule == QCD_SCHED_WAVEFRONT)
     rc = qcd_set_wave_tuning(h, t.chunk_sites, t.passes_per_launch, t.fronts);
+  if (rc == QCD_OK && t.schedule == QCD_SCHED_PAIRS) rc = qcd_set_pair_tuning(h, t.chunk_sites);
   return rc;
 }
 
@@ -861,6 +919,9 @@ int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
   // fronts and chain lengths whose live slices fit in L2
   std::vector<qcd_tuning> cand;
   cand.push_back(qcd_tuning{QCD_SCHED_PHASES, 0, 0, 0, 0.0});
+  // FP32: the fused pairs with the automatic segment and two fixed ones
+  if (h->p.precision == QCD_PREC_FP32)
+    for (int seg : {0, 32, 64}) cand.push_back(qcd_tuning{QCD_SCHED_PAIRS, seg, 0, 0, 0.0});
   int rc = wave_setup(h);
   if (rc) return rc;
   const double slice_bytes = (double)h->g.slice * (6.0 * (h->p.precision == QCD_PREC_FP64 ? 32.0 : 16.0) + 24.0);
@@ -891,6 +952,7 @@ int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
   } bk;
   void *&links_save = bk.links, *&links2_save = bk.links2, *&rng_save = bk.rng, *&acc_save = bk.acc;
   const size_t lb = h->p.precision == QCD_PREC_FP64 ? h->link_bytes / 2 : h->link_bytes;
+  // (the fused pairs swap the FP32 stores: the restore goes to whichever is current then)
   void* lp = h->p.precision == QCD_PREC_FP64 ? (void*)h->lo : (void*)h->q32;
   CUDA_OR_FAIL(h, cudaMalloc(&links_save, lb));
   if (h->p.precision == QCD_PREC_FP64) CUDA_OR_FAIL(h, cudaMalloc(&links2_save, lb));
@@ -905,7 +967,8 @@ int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
   unsigned long long draws_save = 0;
   CUDA_OR_FAIL(h, cudaMemcpyAsync(&draws_save, h->draw_dev, sizeof(draws_save), cudaMemcpyDeviceToHost, h->stream));
   CUDA_OR_FAIL(h, cudaStreamSynchronize(h->stream));
-  const int sched_save = h->sched, chunk_save = h->wave_chunk, chain_save = h->wave_chain, fronts_save = h->wave_fronts;
+  const int sched_save = h->sched, chunk_save = h->wave_chunk, chain_save = h->wave_chain, fronts_save = h->wave_fronts,
+            pseg_save = h->pair_seg;
   cudaEvent_t &e0 = bk.e0, &e1 = bk.e1;
   CUDA_OR_FAIL(h, cudaEventCreate(&e0));
   CUDA_OR_FAIL(h, cudaEventCreate(&e1));
@@ -923,6 +986,7 @@ int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
     if (rc == QCD_OK && cand[i].ms_per_sweep < cand[best].ms_per_sweep) best = (int)i;
   }
   // restore the lattice as it was
+  lp = h->p.precision == QCD_PREC_FP64 ? (void*)h->lo : (void*)h->q32;
   cudaMemcpyAsync(lp, links_save, lb, cudaMemcpyDeviceToDevice, h->stream);
   if (links2_save) cudaMemcpyAsync(h->hi, links2_save, lb, cudaMemcpyDeviceToDevice, h->stream);
   if (rng_save) cudaMemcpyAsync(h->rng, rng_save, rng_bytes, cudaMemcpyDeviceToDevice, h->stream);
@@ -936,6 +1000,7 @@ int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
   h->wave_chunk = chunk_save;
   h->wave_chain = chain_save;
   h->wave_fronts = fronts_save;
+  h->pair_seg = pseg_save;
   if (rc) return rc;
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);

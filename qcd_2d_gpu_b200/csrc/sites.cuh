@@ -84,6 +84,30 @@ __device__ __forceinline__ void site64(const Links64T<CG>& L, const RngStoreT<CG
 // FP32: the same updates with FP32 links and FP64 fix-ups; the heat-bath and
 // Metropolis draw from the counter-based Philox stream of (site, phase), so
 // no generator state is read or written.
+// The new value of FP32 link U_MU at a site of sublattice PAR whose global
+// sublattice index is gid (the Philox site counter and the accept slot);
+// `links` and `n` address the staple links (global memory here, a
+// shared-memory tile in the fused-pair kernel).  Metropolis accept counts are
+// added only when count_accept is set.
+template <int MU, int PAR, int BC, int KIND, class L>
+__device__ __forceinline__ Quat<float> link_update32(const L& links, const Geo& g, const PhaseArgs& a, const Nbr& n,
+                                                     int gid, int renorm, bool count_accept) {
+  Quat<float> A = staple_sum<MU, BC, L, float>(links, g, n, PAR);
+  Quat<float> U;
+  if (KIND == KIND_HB) {
+    PhiloxStream st(a.seed, a.site_off + (unsigned int)gid, draw_phase(a));
+    U = heatbath_fast(A, a.beta, st, a.err);
+  } else if (KIND == KIND_METRO) {
+    PhiloxStream st(a.seed, a.site_off + (unsigned int)gid, draw_phase(a));
+    U = links.ld_own(MU, PAR, n.id);
+    int acc = metropolis_fast(U, A, a.beta, a.eps, a.upd, st);
+    if (count_accept) atomicAdd(a.accept + PAR * g.vh + gid, acc);
+  } else {
+    U = overrelax_fast(A, links.ld_own(MU, PAR, n.id));
+  }
+  return renorm ? renorm_fast(U) : U;
+}
+
 template <int MU, int PAR, int BC, int KIND, bool CG>
 __device__ __forceinline__ void site32(const Links32T<CG>& L, const RngStoreT<CG>& R, const Geo& g,
                                        const PhaseArgs& a, const Nbr& n, int renorm) {

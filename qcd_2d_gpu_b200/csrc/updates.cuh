@@ -22,7 +22,8 @@ namespace qcd {
 enum { KIND_METRO = 0, KIND_HB = 1, KIND_OR = 2 };
 
 // device error word bits
-enum { DEVERR_HB_LOOP = 1, DEVERR_NONUNITARY = 2 };
+// (DEVERR_TIMEOUT: a bounded wait of the wavefront or the fused-pair kernels ran out)
+enum { DEVERR_HB_LOOP = 1, DEVERR_NONUNITARY = 2, DEVERR_TIMEOUT = 4 };
 
 // The Kennedy-Pendleton rejection loop accepts with probability > 1/2 for any
 // staple; this bound is only reached when the staple sum is zero or not

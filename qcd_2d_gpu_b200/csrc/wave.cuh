@@ -28,7 +28,6 @@ namespace qcd {
 constexpr int kMaxWavePhases = 24;
 
 // device error word bit for a wait that ran out
-enum { DEVERR_TIMEOUT = 4 };
 
 struct WaveSched {
   int P;                 // phases in the program

@@ -14,6 +14,10 @@ GPU's hardware cos/log/sincos in the heat-bath against host libm), so:
   sites are counted, and together with the links whose staples they feed in
   the later phases of the pass they must stay below MAX_FLIPPED.
 
+Every check runs with the per-phase launches and with the fused pairs
+(qcd_set_schedule PAIRS), which stage the links in shared memory and
+must give the same updates.
+
 Reference algorithm: functions/mc_updates.h:7-64,109-115 (heat-bath,
 Metropolis, over-relaxation) with the PCC/PMC masks of mc_updates_pcc.h and
 mc_updates_pmc.h:33,40.
@@ -44,10 +48,14 @@ def counter_and_key(L):
     return int(w[-4]) | (int(w[-3]) << 32), int(w[-2]) | (int(w[-1]) << 32)
 
 
-def thermalised(dims, bc, beta, algo="hb", seed=7, **kw):
+SCHEDULES = ["phases", "pairs"]
+
+
+def thermalised(dims, bc, beta, algo="hb", seed=7, schedule="phases", **kw):
     L = q.Lattice(*dims, beta, algo=algo, boundary=bc, precision="fp32", seed=seed, **kw)
     L.init_hot()
     L.sweep(4)
+    L.set_schedule(schedule)  # the pass under test runs with this schedule
     return L
 
 
@@ -55,9 +63,10 @@ def link_dev(a, b):
     return np.abs(a.reshape(-1, 4) - b.reshape(-1, 4)).max(axis=1)
 
 
+@pytest.mark.parametrize("schedule", SCHEDULES)
 @pytest.mark.parametrize("dims,bc", CASES)
-def test_fp32_overrelaxation_pass_matches_oracle(dims, bc):
-    L = thermalised(dims, bc, 7.0)
+def test_fp32_overrelaxation_pass_matches_oracle(dims, bc, schedule):
+    L = thermalised(dims, bc, 7.0, schedule=schedule)
     cfg = L.store_config()
     o = po.Oracle(*dims, 7.0, algo=1, boundary=bc)
     o.load(cfg)
@@ -70,11 +79,12 @@ def test_fp32_overrelaxation_pass_matches_oracle(dims, bc):
     assert d.max() <= OR_TOL, d.max()
 
 
+@pytest.mark.parametrize("schedule", SCHEDULES)
 @pytest.mark.parametrize("dims,bc", CASES)
 @pytest.mark.parametrize("renorm", [False, True])
-def test_fp32_heatbath_pass_matches_oracle(dims, bc, renorm):
+def test_fp32_heatbath_pass_matches_oracle(dims, bc, renorm, schedule):
     beta = 9.0
-    L = thermalised(dims, bc, beta, renorm_every=1 if renorm else 0)
+    L = thermalised(dims, bc, beta, renorm_every=1 if renorm else 0, schedule=schedule)
     cfg = L.store_config()
     ctr, key = counter_and_key(L)
     o = po.Oracle(*dims, beta, algo=1, boundary=bc)
@@ -92,10 +102,11 @@ def test_fp32_heatbath_pass_matches_oracle(dims, bc, renorm):
     assert tries.max() >= 1
 
 
+@pytest.mark.parametrize("schedule", SCHEDULES)
 @pytest.mark.parametrize("dims,bc", CASES[:4])
-def test_fp32_metropolis_pass_matches_oracle(dims, bc):
+def test_fp32_metropolis_pass_matches_oracle(dims, bc, schedule):
     beta, eps, upd = 6.0, 0.3, 3
-    L = thermalised(dims, bc, beta, algo="metro", epsilon=eps, upd=upd)
+    L = thermalised(dims, bc, beta, algo="metro", epsilon=eps, upd=upd, schedule=schedule)
     cfg = L.store_config()
     ctr, key = counter_and_key(L)
     L.accept_reset()
@@ -116,11 +127,12 @@ def test_fp32_metropolis_pass_matches_oracle(dims, bc):
     assert acc_gpu.sum() > 0
 
 
-def test_fp32_sweep_with_overrelaxation_and_renorm_matches_oracle():
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_fp32_sweep_with_overrelaxation_and_renorm_matches_oracle(schedule):
     # the headline sweep's shape on a small PMC lattice: a heat-bath pass, then
     # an over-relaxation pass that re-projects each link as it stores it
     dims, bc, beta = (12, 10, 14), 2, 10.0
-    L = thermalised(dims, bc, beta, n_or=1, renorm_every=1)
+    L = thermalised(dims, bc, beta, n_or=1, renorm_every=1, schedule=schedule)
     cfg = L.store_config()
     ctr, key = counter_and_key(L)
     o = po.Oracle(*dims, beta, algo=1, boundary=bc)
