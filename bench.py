@@ -416,6 +416,8 @@ def main():
     ap.add_argument("--lattice", type=int, nargs=3, default=None, help="override (testing only)")
     ap.add_argument("--workload", default="sweep", choices=["sweep", "accuracy", "c3-accuracy"])
     ap.add_argument("--schedule", default="auto", choices=["auto", "phases", "wavefront", "pairs"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
+                    help="link precision of the timed workload (fp32 is the benchmark; fp64 for profiling)")
     ap.add_argument("--wave-tuning", type=int, nargs=3, default=None, metavar=("CHUNK", "PASSES", "FRONTS"))
     ap.add_argument("--scan-size", type=int, default=128)
     ap.add_argument("--scan-sweeps", type=int, default=2000)
@@ -464,7 +466,8 @@ def main():
     torch.cuda.set_stream(stream)
     V = LT * LX * LY
 
-    L = q.Lattice(LT, LX, LY, BETA, algo="hb", boundary="pmc", precision="fp32", n_or=N_OR,
+    PREC = args.precision
+    L = q.Lattice(LT, LX, LY, BETA, algo="hb", boundary="pmc", precision=PREC, n_or=N_OR,
                   renorm_every=1, seed=1234 + rank)
     L.set_stream(stream.cuda_stream)
     L.set_schedule(args.schedule)
@@ -506,12 +509,12 @@ def main():
     # launches of one pass: six phase kernels (the wavefront runs passes in
     # persistent launches); the re-projection rides on the last pass, the
     # measurement is one launch
-    per_pass = {"phases": 6}.get(L_schedule)
+    per_pass = {"phases": 6, "pairs": 3}.get(L_schedule)
     # + one one-thread launch per heat-bath pass advancing the FP32 draws' counter
     launches_per_step = N_COR * (per_pass * (1 + N_OR) + 1) + 1 if per_pass else None
 
     # ---- dominant kernel: the over-relaxation pass, timed live -----------
-    # one qcd_overrelax pass = 6 phase launches
+    # one qcd_overrelax pass = 6 phase launches (3 fused-pair launches)
     reps = 5
     a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a0.record(stream)
@@ -520,7 +523,7 @@ def main():
     b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     L.close()
-    L2h = q.Lattice(LT, LX, LY, BETA, algo="hb", boundary="pmc", precision="fp32", n_or=0, seed=99)
+    L2h = q.Lattice(LT, LX, LY, BETA, algo="hb", boundary="pmc", precision=PREC, n_or=0, seed=99)
     L2h.set_stream(stream.cuda_stream)
     L2h.set_schedule(args.schedule)
     if args.wave_tuning:
@@ -540,17 +543,22 @@ def main():
     # strict algorithmic bytes: each FP32 link read once and written once per
     # pass, 32 B per update (the FP32 heat-bath draws keep no generator state);
     # a pass is 3V updates
-    or_bytes = 32.0 * 3 * V / n_launch
-    hb_bytes = 32.0 * 3 * V / n_launch
+    # (FP64: 2 x 32 B per update, and the heat-bath reads and writes its site's
+    # 24-B MRG32k3a state once per six updates)
+    link_b = 16.0 if PREC == "fp32" else 32.0
+    or_bytes = 2 * link_b * 3 * V / n_launch
+    hb_bytes = (2 * link_b + (0.0 if PREC == "fp32" else 2 * 24.0 / 6)) * 3 * V / n_launch
     hbm, peak_kind = peaks()
     or_gbs = or_bytes / (or_launch_ms * 1e-3) / 1e9
-    roofline = {"kernel": "phase32<mu, par, PMC, OR> (over-relaxation phase)", "bound": "hbm", "achieved": or_gbs,
+    kname = ("pair32<mu, PMC, OR> (fused over-relaxation pair)" if L_schedule == "pairs"
+             else f"phase{PREC[2:]}<mu, par, PMC, OR> (over-relaxation phase)")
+    roofline = {"kernel": kname, "bound": "hbm", "achieved": or_gbs,
                 "peak": hbm, "unit": "GB/s", "frac": or_gbs / hbm, "peak_source": peak_kind,
                 "traffic": None, "algorithmic_bytes_per_launch": or_bytes, "launch_ms": or_launch_ms,
                 "launches_per_pass": n_launch,
                 "heatbath": {"launch_ms": hb_launch_ms, "achieved": hb_bytes / (hb_launch_ms * 1e-3) / 1e9}}
     traffic_file = os.path.join(ROOT, "profiles", "dram_traffic.json")
-    if os.path.exists(traffic_file):
+    if os.path.exists(traffic_file) and PREC == "fp32" and L_schedule == "phases":
         try:
             roofline["traffic"] = json.load(open(traffic_file)).get("phase32_or_bytes_per_launch")
         except Exception:
@@ -578,7 +586,7 @@ def main():
     hv = host_cfg.numpy()
     hv[:] = 0.0
     hv[0::4] = 1.0  # a cold configuration
-    E = q.Lattice(LT, LX, LY, BETA, algo="hb", boundary="pmc", precision="fp32", n_or=N_OR,
+    E = q.Lattice(LT, LX, LY, BETA, algo="hb", boundary="pmc", precision=PREC, n_or=N_OR,
                   renorm_every=1, seed=4321 + rank)
     E.set_stream(stream.cuda_stream)
     E.load_config(hv)  # allocate the staging buffer outside the timed region
@@ -622,12 +630,14 @@ def main():
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32+f64-fixups",
+            "dtype": "f32+f64-fixups" if PREC == "fp32" else "f64",
             "data": "synthetic (hot start from seeded MRG32k3a streams; FP32 draws from Philox4x32-10)",
             "config": {"workload": f"{LT}x{LX}x{LY} PMC, hot start, sweep = 1 heat-bath + {N_OR} "
-                                   f"over-relaxation, FP32 links + FP64 fix-ups, renormalise every sweep, "
+                                   f"over-relaxation, "
+                                   + ("FP32 links + FP64 fix-ups, " if PREC == "fp32" else "FP64 links, ")
+                                   + "renormalise every sweep, "
                                    f"measure every {N_COR} sweeps",
-                       "lattice": [LT, LX, LY], "boundary": "pmc", "precision": "fp32", "n_or": N_OR,
+                       "lattice": [LT, LX, LY], "boundary": "pmc", "precision": PREC, "n_or": N_OR,
                        "n_cor": N_COR, "beta": BETA,
                        "l2": f"inputs larger than L2 ({V * 48 / 1e9:.2f} GB FP32 link store)",
                        "parallelism": f"replicas x{ws}"},

@@ -231,7 +231,9 @@ void qcd_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4
 /* Lattice facts. */
 long long qcd_volume(const qcd_lattice* h);
 int qcd_get_params(const qcd_lattice* h, qcd_params* out);
-/* Device pointer and byte size of the link store (diagnostics, benchmarks). */
+/* Device pointer and byte size of the current link store (diagnostics,
+   benchmarks).  Under QCD_SCHED_PAIRS each pass moves the links to the other
+   of two stores, so the pointer holds until the next sweep. */
 int qcd_link_store(const qcd_lattice* h, void** dev_ptr, size_t* bytes);
 
 const char* qcd_last_error(const qcd_lattice* h);

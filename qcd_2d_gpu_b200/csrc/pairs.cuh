@@ -13,11 +13,13 @@
 // recomputed by each CTA that needs them (their inputs are old links, so the
 // recomputation is exact).
 //
-// Data flow per CTA (one per SM; 226 KB of shared memory):
+// Data flow per CTA (one per SM; 227 KB of shared memory):
 //   * seven planes of NS x NR x W float4: the six link classes (direction,
-//     parity) of NS consecutive slices of the tile and its halo, filled row by
-//     row with cp.async.bulk from HBM/L2, and the new even U_MU of the same
-//     slices;
+//     parity) of NS consecutive slices of the tile and its halo, each slice of
+//     a class one tensor copy (cp.async.bulk.tensor, a 5-D box of the link
+//     store) from HBM/L2, and the new even U_MU of the same slices; boxes that
+//     cross the lattice edge read zeros there and the CTA patches those cells
+//     with their periodic images;
 //   * NS mbarriers, one per slice slot; a slot is refilled with the slice NS
 //     ahead once the block barrier shows nobody reads it, so every load is
 //     issued two steps before it is needed;
@@ -29,9 +31,12 @@
 // draws: the Philox counter is the site's global sublattice index and the
 // phase number), the staples now gathered from shared memory.
 //
-// Bulk copies need 16-byte aligned addresses and sizes: links are float4 and
-// the stores come from cudaMalloc.  No copy uses cluster multicast.
+// Tensor copies: the innermost coordinate is the quaternion component, always
+// 0, so every box starts on a 16-byte boundary; the store comes from
+// cudaMalloc and each slot is padded to 128 bytes.  No copy uses cluster
+// multicast.
 #pragma once
+#include <cuda.h>
 #include <stdint.h>
 #include "sites.cuh"
 
@@ -41,10 +46,14 @@ constexpr int kPairNS = 7;      // slice slots
 constexpr int kPairNR = 17;     // staged rows
 constexpr int kPairW = 17;      // staged y' window
 constexpr int kPairPlanes = 7;  // six link classes + the new even links of MU
-constexpr int kPairPlane = kPairNS * kPairNR * kPairW;  // float4 per plane
-constexpr int kPairSlotStride = kPairNR * kPairW;       // float4 per slot of a plane
+// float4 per slot of a plane: the NR x W box of one slice, padded to 128 bytes
+// (the alignment of a tensor copy's shared-memory destination)
+constexpr int kPairSlotStride = (kPairNR * kPairW + 7) / 8 * 8;
+constexpr int kPairPlane = kPairNS * kPairSlotStride;  // float4 per plane
 constexpr size_t kPairSmemBytes = (size_t)kPairPlanes * kPairPlane * sizeof(float4) + kPairNS * sizeof(uint64_t);
 constexpr unsigned int kPairFillBytes = 6u * kPairNR * kPairW * sizeof(float4);  // one slice of six classes
+// within the 227 KB a block may opt in to, with room for the static variables
+static_assert(kPairSmemBytes + 256 <= 232448, "pair kernel shared memory");
 constexpr unsigned long long kPairWaitNs = 200000000ull;  // bound of one wait: 0.2 s, far above any real load
 
 // Frame of the pair kernel for direction MU.
@@ -83,6 +92,7 @@ struct PairPlanes {
   const float4* src[6];  // the current link classes, plane d*2 + p
   float4* dst_e;         // U_MU(even) of the other store
   float4* dst_o;         // U_MU(odd) of the other store
+  int alt_mask;          // bit p: class p is read from the second store (tensor map tm_alt)
 };
 
 struct PairGrid {
@@ -144,12 +154,15 @@ __device__ __forceinline__ void mbar_drain(uint64_t* bar, unsigned int parity) {
   while (!mbar_test(addr, parity) && global_ns() - t0 < kPairWaitNs) {
   }
 }
-// bytes (a multiple of 16) from global src to shared dst, completing on bar
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned int bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
+// One box of a 5-D tensor map (component, y', x, t, class) into shared memory,
+// completing on bar.  Coordinates outside the tensor read as zero.
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, int c1, int c2, int c3, int c4,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+      : "memory");
 }
 
 // The links of a step as the staple gather sees them: plane d*2 + p of the
@@ -165,48 +178,94 @@ struct PairSmem {
   __device__ __forceinline__ Quat<float> ld_own(int dir, int par, int idx) const { return ld(dir, par, idx); }
 };
 
-// Fill slot `slot` with unwrapped slice sx of the tile's rows and window:
-// 6 classes x NR rows, each row one or (where the window wraps) more bulk
-// copies.  Called by all 32 lanes of one warp.
+// Fill slot `slot` with unwrapped slice sx of the tile's rows and window: one
+// tensor copy per link class (the box NR rows x W y' of one slice), issued by
+// one thread.  Rows and y' are given unwrapped: where the box crosses the
+// lattice edge it reads zeros, and the CTA patches those cells (pair_patch).
 template <int MU>
 __device__ __forceinline__ void pair_fill(float4* sm, uint64_t* bar, int slot, int sx, const PairPlanes& P,
-                                          const Geo& g, int R0, int Y0h, int lane) {
+                                          const CUtensorMap* tm_cur, const CUtensorMap* tm_alt, const Geo& g,
+                                          int R0, int Y0h) {
   typedef PairCfg<MU> C;
-  const int ls = C::S == DIR_T ? g.lt : g.lx, lrow = C::ROW == DIR_T ? g.lt : g.lx;
+  const int ls = C::S == DIR_T ? g.lt : g.lx;
   const int s = pmod(sx, ls);
-  if (lane == 0) {
-    // the generic-proxy reads of this slot (before the block barrier) come
-    // before the asynchronous writes that refill it
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(bar, kPairFillBytes);
-  }
-  __syncwarp();
-  if (lane < kPairNR) {
-    const int r = lane;
-    const int gr = pmod(R0 - C::ROW0 + r, lrow);
-    const int t = C::S == DIR_T ? s : gr, x = C::S == DIR_T ? gr : s;
-    const size_t row_off = (size_t)g.lyh * (size_t)(x + g.lx * t);
-    const int y0 = pmod(Y0h - C::W0, g.lyh);
+  const int row0 = R0 - C::ROW0, y0 = Y0h - C::W0;
+  const int cx = C::S == DIR_T ? row0 : s, ct = C::S == DIR_T ? s : row0;
+  // the generic-proxy reads of this slot (before the block barrier) come
+  // before the asynchronous writes that refill it
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  mbar_expect_tx(bar, kPairFillBytes);
 #pragma unroll
-    for (int p = 0; p < 6; p++) {
-      const float4* src = P.src[p] + row_off;
-      float4* dst = sm + p * kPairPlane + slot * kPairSlotStride + r * kPairW;
-      int w = 0, y = y0;
-      while (w < kPairW) {
-        const int n = min(kPairW - w, g.lyh - y);
-        bulk_load(dst + w, src + y, (unsigned int)n * 16u, bar);
-        w += n;
-        y = 0;
-      }
+  for (int p = 0; p < 6; p++)
+    tma_load_5d(sm + p * kPairPlane + slot * kPairSlotStride, (P.alt_mask >> p) & 1 ? tm_alt : tm_cur, y0, cx, ct,
+                p, bar);
+}
+
+// The cells of a staged slice that lie beyond the lattice edge in the rows or
+// in y' (the box read zeros there), with their periodic images: up to four
+// per thread, fixed for the CTA except for the slice.
+struct PairPatch {
+  const float4* src[4];  // link of the image in its class, slice term excluded
+  int soff[4];           // shared-memory index without the slot term
+  int valid;             // bit m: cell m is an edge cell
+};
+
+// Cell m of this thread is k = tid + m * NT of the 6 x NR x W cells of a slice
+// (every cell has a thread: 6 * 17 * 17 <= 4 * 448).
+template <int MU>
+__device__ __forceinline__ PairPatch pair_patch_cells(const PairPlanes& P, const Geo& g, int R0, int Y0h, int tid) {
+  typedef PairCfg<MU> C;
+  static_assert(6 * kPairNR * kPairW <= 4 * C::NT, "patch cells per thread");
+  const int lrow = C::ROW == DIR_T ? g.lt : g.lx;
+  PairPatch pp;
+  pp.valid = 0;
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    pp.src[m] = P.src[0];
+    pp.soff[m] = 0;
+    const int k = tid + m * C::NT;
+    if (k >= 6 * kPairNR * kPairW) continue;
+    const int p = k / (kPairNR * kPairW), rem = k - p * (kPairNR * kPairW);
+    const int r = rem / kPairW, w = rem - r * kPairW;
+    const int gr_u = R0 - C::ROW0 + r, y_u = Y0h - C::W0 + w;
+    if (gr_u >= 0 && gr_u < lrow && y_u >= 0 && y_u < g.lyh) continue;
+    const int gr = pmod(gr_u, lrow), yq = pmod(y_u, g.lyh);
+    // the row coordinate is x (slice = t) or t (slice = x)
+    const size_t off = C::S == DIR_T ? (size_t)yq + (size_t)g.lyh * gr : (size_t)yq + (size_t)g.lyh * g.lx * gr;
+    const float4* base = P.src[0];
+    switch (p) {
+      case 1: base = P.src[1]; break;
+      case 2: base = P.src[2]; break;
+      case 3: base = P.src[3]; break;
+      case 4: base = P.src[4]; break;
+      case 5: base = P.src[5]; break;
+      default: break;
     }
+    pp.src[m] = base + off;
+    pp.soff[m] = p * kPairPlane + r * kPairW + w;
+    pp.valid |= 1 << m;
   }
+  return pp;
+}
+
+// Overwrite the thread's edge cells of slot `slot` (unwrapped slice sx) with
+// their periodic images, after the slot's tensor copies completed.
+template <int MU>
+__device__ __forceinline__ void pair_patch(float4* sm, const PairPatch& pp, int slot, int sx, const Geo& g) {
+  typedef PairCfg<MU> C;
+  const int ls = C::S == DIR_T ? g.lt : g.lx;
+  const size_t sterm = C::S == DIR_T ? (size_t)pmod(sx, ls) * g.lyh * g.lx : (size_t)pmod(sx, ls) * g.lyh;
+#pragma unroll
+  for (int m = 0; m < 4; m++)
+    if ((pp.valid >> m) & 1) sm[pp.soff[m] + slot * kPairSlotStride] = __ldcg(pp.src[m] + sterm);
 }
 
 // One fused pair (MU, even) + (MU, odd) over one segment of the streamed
 // direction for one tile.  Grid: (row tiles x y tiles, segments).
 template <int MU, int BC, int KIND>
 __global__ void __launch_bounds__(PairCfg<MU>::NT, 1)
-    pair32(PairPlanes P, Geo g, PhaseArgs a, PairGrid pg) {
+    pair32(const __grid_constant__ CUtensorMap tm_cur, const __grid_constant__ CUtensorMap tm_alt, PairPlanes P,
+           Geo g, PhaseArgs a, PairGrid pg) {
   typedef PairCfg<MU> C;
   extern __shared__ __align__(128) float4 sm[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kPairPlanes * kPairPlane);
@@ -218,7 +277,7 @@ __global__ void __launch_bounds__(PairCfg<MU>::NT, 1)
   const int nr = min(C::TR, lrow - R0), ny = min(C::TY, g.lyh - Y0h);
   const int s0 = blockIdx.y * pg.seg, s1 = min(s0 + pg.seg, ls);
   const int first = s0 - 2, last = s1 + 1;  // unwrapped slices staged
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x;
 
   if (tid == 0) {
     abort_flag = 0;
@@ -226,9 +285,16 @@ __global__ void __launch_bounds__(PairCfg<MU>::NT, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  if (warp == 0)
+  if (tid == 0)
     for (int x = first; x <= last && x < first + kPairNS; x++)
-      pair_fill<MU>(sm, &bars[x - first], x - first, x, P, g, R0, Y0h, lane);
+      pair_fill<MU>(sm, &bars[x - first], x - first, x, P, &tm_cur, &tm_alt, g, R0, Y0h);
+  // a tile whose staged rows or y' window cross the lattice edge patches the
+  // cells its boxes read as zeros
+  const bool edge = R0 - C::ROW0 < 0 || R0 - C::ROW0 + kPairNR > lrow || Y0h - C::W0 < 0 ||
+                    Y0h - C::W0 + kPairW > g.lyh;
+  PairPatch pp;
+  pp.valid = 0;
+  if (edge) pp = pair_patch_cells<MU>(P, g, R0, Y0h, tid);
 
   // this thread's item: an even site (tile + ring) or an odd site (tile)
   const int ne_row = C::YRING ? ny + 1 : ny;                  // even items per row
@@ -262,6 +328,14 @@ __global__ void __launch_bounds__(PairCfg<MU>::NT, 1)
     if (!ok) {
       atomicOr(a.err, DEVERR_TIMEOUT);
       abort_flag = 1;
+    }
+    if (edge) {
+      if (ok) {
+        if (j == 0)
+          for (int x = first; x <= e; x++) pair_patch<MU>(sm, pp, (x - first) % kPairNS, x, g);
+        if (e + 1 <= last) pair_patch<MU>(sm, pp, (e + 1 - first) % kPairNS, e + 1, g);
+      }
+      __syncthreads();
     }
     if (ok && (is_even || is_odd)) {
       // slice of this thread's update and its slot
@@ -328,7 +402,8 @@ __global__ void __launch_bounds__(PairCfg<MU>::NT, 1)
     // the slot of slice e - 3 is free: refill it with slice e - 3 + NS
     const int fx = e - 3 + kPairNS;
     if (e - 3 >= first && fx <= last) {
-      if (warp == 0) pair_fill<MU>(sm, &bars[(fx - first) % kPairNS], (fx - first) % kPairNS, fx, P, g, R0, Y0h, lane);
+      if (tid == 0)
+        pair_fill<MU>(sm, &bars[(fx - first) % kPairNS], (fx - first) % kPairNS, fx, P, &tm_cur, &tm_alt, g, R0, Y0h);
       issued = fx;
     }
   }

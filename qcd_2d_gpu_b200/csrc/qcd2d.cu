@@ -66,6 +66,10 @@ struct qcd_lattice {
   int wave_tasks_chunk[5] = {0, 0, 0, 0, 0};
   int wave_tasks_fronts[5] = {0, 0, 0, 0, 0};
   int sms = 0;       // multiprocessors of the device (fused pairs)
+  // fused pairs: the two FP32 stores and their tensor maps (pair_buf[0] is
+  // the store allocated at create; q32 / q32alt point at one each)
+  float4* pair_buf[2] = {nullptr, nullptr};
+  PairMaps pair_maps[2];
   int pair_seg = 0;  // fused pairs: streamed slices per CTA (0: automatic)
   char msg[512] = {0};
 };
@@ -455,7 +459,19 @@ bool use_pairs(const qcd_lattice* h) { return h->sched == QCD_SCHED_PAIRS && h->
 // when the schedule is chosen, never inside a pass, so that passes can be
 // captured in a CUDA graph).
 int pairs_setup(qcd_lattice* h) {
-  if (!h->q32alt) CUDA_OR_FAIL(h, cudaMalloc(&h->q32alt, h->link_bytes));
+  if (!h->q32alt) {
+    CUDA_OR_FAIL(h, cudaMalloc(&h->q32alt, h->link_bytes));
+    h->pair_buf[0] = h->q32;
+    h->pair_buf[1] = h->q32alt;
+    for (int b = 0; b < 2; b++) {
+      cudaError_t e = pair_encode_maps(h->pair_buf[b], h->g, &h->pair_maps[b]);
+      if (e != cudaSuccess) {
+        cudaFree(h->q32alt);
+        h->q32alt = nullptr;
+        return fail(h, QCD_ERR_UNSUPPORTED, "fused pairs: tensor maps of the link store: %s", cudaGetErrorString(e));
+      }
+    }
+  }
   if (!h->sms) {
     int dev = 0;
     CUDA_OR_FAIL(h, cudaGetDevice(&dev));
@@ -469,7 +485,9 @@ int pairs_setup(qcd_lattice* h) {
 int pass_pairs(qcd_lattice* h, int kind, int renorm) {
   if (!h->q32alt || !h->sms) return fail(h, QCD_ERR_INVALID, "fused pairs used before their setup");
   PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, renorm, h->draw_key, h->draw_dev, 0, 0};
-  CUDA_OR_FAIL(h, pair_pass32(h->q32, h->q32alt, h->g, h->p.boundary, kind, a, h->pair_seg, h->sms, h->stream));
+  const PairMaps& mc = h->pair_maps[h->q32 == h->pair_buf[0] ? 0 : 1];
+  const PairMaps& ma = h->pair_maps[h->q32 == h->pair_buf[0] ? 1 : 0];
+  CUDA_OR_FAIL(h, pair_pass32(h->q32, h->q32alt, mc, ma, h->g, h->p.boundary, kind, a, h->pair_seg, h->sms, h->stream));
   float4* t = h->q32;
   h->q32 = h->q32alt;
   h->q32alt = t;
