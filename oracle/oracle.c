@@ -757,10 +757,12 @@ static int metropolis32(fquat* U, fquat A, float beta, float eps, int upd, pstre
   return acc;
 }
 
-/* mc_updates.h:109-115 in float */
+/* mc_updates.h:109-115 in float, in the library's form: U' = 2 (<A, Ubar> /
+ * |A|^2) Abar - U, which is (Ahat U Ahat)^+ by the quaternion identity
+ * q p q = 2 <q, pbar> q - |q|^2 pbar */
 static fquat over_relaxation32(fquat A, fquat U) {
-  A = f_scale(A, 1.0f / sqrtf(f_det(A)));
-  return f_mul_ad(A, f_mul_adbd(U, A));
+  const float c = 2.f * (A.w * U.w - A.x * U.x - A.y * U.y - A.z * U.z) / f_det(A);
+  return (fquat){c * A.w - U.w, -c * A.x - U.x, -c * A.y - U.y, -c * A.z - U.z};
 }
 
 /* re-projection with the norm taken in double */

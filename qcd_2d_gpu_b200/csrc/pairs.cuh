@@ -316,9 +316,33 @@ __global__ void __launch_bounds__(PairCfg<MU>::NT, 1)
   const bool tile_row = r >= C::ROW0 && r < C::ROW0 + nr;
   int issued = min(last, first + kPairNS - 1);  // last slice whose fill was issued
 
+  // Per-thread state along the stream, advanced by one slice per step: the
+  // unwrapped slice of this thread's update, its slot, its global slice, the
+  // parity q of its physical y (which flips from slice to slice) and the
+  // global index term of the slice.  The window column, y' and tile test take
+  // one of two values, for q = 0 and q = 1.
+  const int par = is_even ? 0 : 1;
+  int sx = is_even ? s0 - 1 : s0 - 3;
+  int slot = pmod(sx - first, kPairNS);
+  int gs = pmod(sx, ls);
+  int q = ((sx + grow) & 1) ^ par;
+  const int s_stride = C::S == DIR_T ? g.lyh * g.lx : g.lyh;
+  int s_term = gs * s_stride;
+  const int row_term = C::S == DIR_T ? g.lyh * grow : g.lyh * g.lx * grow;
+  // window column: even items of a y-ring row start one column early when
+  // their physical y is odd
+  const int w_0 = C::YRING ? C::W0 + i : i;
+  const int w_1 = C::YRING ? (is_even ? C::W0 - 1 + i : C::W0 + i) : i;
+  const int yq_0 = pmod(Y0h - C::W0 + w_0, g.lyh), yq_1 = pmod(Y0h - C::W0 + w_1, g.lyh);
+  const bool in_tile_0 = C::YRING ? (w_0 >= C::W0 && w_0 < C::W0 + ny) : tile_row;
+  const bool in_tile_1 = C::YRING ? (w_1 >= C::W0 && w_1 < C::W0 + ny) : tile_row;
+  const int row_off = r * kPairW;
+  PhaseArgs ap = a;
+  ap.phase_off = a.phase_off + (unsigned int)par;
+
   const int J = s1 - s0 + 3;
   for (int j = 0; j < J; j++) {
-    const int e = s0 - 1 + j, o = e - 2;
+    const int e = s0 - 1 + j;
     // wait for the slices first read at this step
     bool ok = true;
     if (j == 0) {
@@ -337,65 +361,60 @@ __global__ void __launch_bounds__(PairCfg<MU>::NT, 1)
       }
       __syncthreads();
     }
-    if (ok && (is_even || is_odd)) {
-      // slice of this thread's update and its slot
-      const int sx = is_even ? e : o;
-      const bool active = is_even ? (e <= s1) : (o >= s0);
-      if (active) {
-        const int slot = (sx - first) % kPairNS;
-        const int gs = pmod(sx, ls);
-        const int par = is_even ? 0 : 1;
-        // parity of the physical y of sublattice `par` on this row of slice sx
-        const int q = ((sx + grow) & 1) ^ par;
-        // window column: even items of a y-ring row start one column early
-        // when their physical y is odd
-        const int w = C::YRING ? (is_even ? C::W0 - q + i : C::W0 + i) : i;
-        const int yq = pmod(Y0h - C::W0 + w, g.lyh);
-        const int t = C::S == DIR_T ? gs : grow, xg = C::S == DIR_T ? grow : gs;
-        const int gid = yq + g.lyh * (xg + g.lx * t);
-        Nbr n;
-        n.id = slot * kPairSlotStride + r * kPairW + w;
-        n.yq = yq;
-        n.q = q;
-        n.x = xg;
-        n.t = t;
-        n.yp = q ? 1 : 0;
-        n.ym = q ? 0 : -1;
-        const int sp = slot == kPairNS - 1 ? -(kPairNS - 1) * kPairSlotStride : kPairSlotStride;
-        const int sm_ = slot == 0 ? (kPairNS - 1) * kPairSlotStride : -kPairSlotStride;
-        if (C::ROW == DIR_X) {
-          n.xp = kPairW;
-          n.xm = -kPairW;
-          n.tp = sp;
-          n.tm = sm_;
-        } else {
-          n.tp = kPairW;
-          n.tm = -kPairW;
-          n.xp = sp;
-          n.xm = sm_;
-        }
-        const bool in_tile = C::YRING ? (w >= C::W0 && w < C::W0 + ny) : tile_row;
-        const bool in_seg = sx >= s0 && sx < s1;
-        PhaseArgs ap = a;
-        ap.phase_off = a.phase_off + (unsigned int)par;
-        Quat<float> U;
-        if (is_even) {
-          const PairSmem<MU, false> L{sm};
-          if (BC == BC_PCC && MU != DIR_Y && at_y0(g, n))
-            U = L.ld_own(MU, 0, n.id);  // frozen: the old link carries over
-          else
-            U = link_update32<MU, 0, BC, KIND>(L, g, ap, n, gid, a.renorm, in_tile && in_seg);
-          sm[6 * kPairPlane + n.id] = make_float4(U.w, U.x, U.y, U.z);
-          if (in_tile && in_seg) P.dst_e[gid] = make_float4(U.w, U.x, U.y, U.z);
-        } else {
-          const PairSmem<MU, true> L{sm};
-          if (BC == BC_PCC && MU != DIR_Y && at_y0(g, n))
-            U = L.ld_own(MU, 1, n.id);
-          else
-            U = link_update32<MU, 1, BC, KIND>(L, g, ap, n, gid, a.renorm, true);
-          P.dst_o[gid] = make_float4(U.w, U.x, U.y, U.z);
-        }
+    const bool active = is_even ? (sx <= s1) : (is_odd && sx >= s0);
+    if (ok && active) {
+      const int w = q ? w_1 : w_0, yq = q ? yq_1 : yq_0;
+      const int gid = yq + row_term + s_term;
+      Nbr n;
+      n.id = slot * kPairSlotStride + row_off + w;
+      n.yq = yq;
+      n.q = q;
+      n.x = 0;
+      n.t = 0;
+      n.yp = q ? 1 : 0;
+      n.ym = q ? 0 : -1;
+      const int sp = slot == kPairNS - 1 ? -(kPairNS - 1) * kPairSlotStride : kPairSlotStride;
+      const int sm_ = slot == 0 ? (kPairNS - 1) * kPairSlotStride : -kPairSlotStride;
+      if (C::ROW == DIR_X) {
+        n.xp = kPairW;
+        n.xm = -kPairW;
+        n.tp = sp;
+        n.tm = sm_;
+      } else {
+        n.tp = kPairW;
+        n.tm = -kPairW;
+        n.xp = sp;
+        n.xm = sm_;
       }
+      const bool in_tile = q ? in_tile_1 : in_tile_0;
+      const bool in_seg = sx >= s0 && sx < s1;
+      Quat<float> U;
+      if (is_even) {
+        const PairSmem<MU, false> L{sm};
+        if (BC == BC_PCC && MU != DIR_Y && at_y0(g, n))
+          U = L.ld_own(MU, 0, n.id);  // frozen: the old link carries over
+        else
+          U = link_update32<MU, 0, BC, KIND>(L, g, ap, n, gid, a.renorm, in_tile && in_seg);
+        sm[6 * kPairPlane + n.id] = make_float4(U.w, U.x, U.y, U.z);
+        if (in_tile && in_seg) P.dst_e[gid] = make_float4(U.w, U.x, U.y, U.z);
+      } else {
+        const PairSmem<MU, true> L{sm};
+        if (BC == BC_PCC && MU != DIR_Y && at_y0(g, n))
+          U = L.ld_own(MU, 1, n.id);
+        else
+          U = link_update32<MU, 1, BC, KIND>(L, g, ap, n, gid, a.renorm, true);
+        P.dst_o[gid] = make_float4(U.w, U.x, U.y, U.z);
+      }
+    }
+    // the next slice
+    sx++;
+    q ^= 1;
+    if (++slot == kPairNS) slot = 0;
+    if (++gs == ls) {
+      gs = 0;
+      s_term = 0;
+    } else {
+      s_term += s_stride;
     }
     __syncthreads();
     if (abort_flag) break;

@@ -36,6 +36,33 @@ struct Planes {
   static constexpr int NU2 = MU == DIR_T ? DIR_X : DIR_T;
 };
 
+// FP32 staples add their second product straight into the sum with
+// multiply-adds (A + X Y^+, A + X Y); FP64 keeps the reference's separate
+// product and sum, whose rounding the bit-parity tests pin.
+__device__ __forceinline__ Quat<float> q_acc_mul_bd(const Quat<float>& A, const Quat<float>& a, const Quat<float>& b) {
+  Quat<float> c;
+  c.w = A.w + a.w * b.w + a.x * b.x + a.y * b.y + a.z * b.z;
+  c.x = A.x + a.x * b.w - a.w * b.x - a.y * b.z + a.z * b.y;
+  c.y = A.y + a.y * b.w - a.z * b.x - a.w * b.y + a.x * b.z;
+  c.z = A.z + a.z * b.w + a.y * b.x - a.w * b.z - a.x * b.y;
+  return c;
+}
+__device__ __forceinline__ Quat<float> q_acc_mul(const Quat<float>& A, const Quat<float>& a, const Quat<float>& b) {
+  Quat<float> c;
+  c.w = A.w + a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z;
+  c.x = A.x + a.x * b.w + a.w * b.x + a.y * b.z - a.z * b.y;
+  c.y = A.y + a.y * b.w + a.z * b.x + a.w * b.y - a.x * b.z;
+  c.z = A.z + a.z * b.w - a.y * b.x + a.w * b.z + a.x * b.y;
+  return c;
+}
+__device__ __forceinline__ Quat<double> q_acc_mul_bd(const Quat<double>& A, const Quat<double>& a,
+                                                     const Quat<double>& b) {
+  return q_add(A, q_mul_bd(a, b));
+}
+__device__ __forceinline__ Quat<double> q_acc_mul(const Quat<double>& A, const Quat<double>& a, const Quat<double>& b) {
+  return q_add(A, q_mul(a, b));
+}
+
 template <int MU, int NU, int BC, class L, class R>
 __device__ __forceinline__ void add_staples(const L& links, const Geo& g, const Nbr& n, int par,
                                             Quat<R>& A) {
@@ -46,14 +73,14 @@ __device__ __forceinline__ void add_staples(const L& links, const Geo& g, const 
     Quat<R> a = links.ld(NU, o, n.id + off_plus(n, MU));
     Quat<R> b = links.ld(MU, o, n.id + off_plus(n, NU));
     Quat<R> c = links.ld(NU, par, n.id);
-    A = q_add(A, q_mul_bd(q_mul_bd(a, b), c));
+    A = q_acc_mul_bd(A, q_mul_bd(a, b), c);
   }
   if (!drop_bwd) {
     const int m = n.id + off_minus(n, NU);
     Quat<R> a = links.ld(NU, par, m + off_plus(n, MU));
     Quat<R> b = links.ld(MU, o, m);
     Quat<R> c = links.ld(NU, o, m);
-    A = q_add(A, q_mul(q_mul_adbd(a, b), c));
+    A = q_acc_mul(A, q_mul_adbd(a, b), c);
   }
 }
 
@@ -188,10 +215,15 @@ __device__ __forceinline__ Quat<float> heatbath_fast(Quat<float> A, float beta, 
   return q_mul_bd(X, A);
 }
 
-__device__ __forceinline__ Quat<float> overrelax_fast(Quat<float> A, const Quat<float>& U) {
-  float rinv = rsqrtf(q_det(A));
-  A = Quat<float>{A.w * rinv, A.x * rinv, A.y * rinv, A.z * rinv};
-  return q_mul_ad(A, q_mul_adbd(U, A));
+// Over-relaxation U -> (Ahat U Ahat)^+, Ahat = A/|A| (mc_updates.h:109-115),
+// written with the quaternion identity q p q = 2 <q, pbar> q - |q|^2 pbar:
+//   U' = 2 (<A, Ubar> / |A|^2) Abar - U,   <A, Ubar> = 1/2 Re tr(U A),
+// the same map as the reference's two products with ~16 operations instead of
+// ~41; it keeps <A, Ubar> (the local action) and |U'| = |U| exactly in exact
+// arithmetic.  FP32 only: the FP64 path keeps the reference's products.
+__device__ __forceinline__ Quat<float> overrelax_fast(const Quat<float>& A, const Quat<float>& U) {
+  const float c = __fdividef(2.f * q_retr_mul(A, U), q_det(A));
+  return Quat<float>{c * A.w - U.w, -c * A.x - U.x, -c * A.y - U.y, -c * A.z - U.z};
 }
 
 // Metropolis with FP32 links: proposal and action change in float, the
