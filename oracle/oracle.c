@@ -569,8 +569,8 @@ int ora_get_threads(void) {
  * has FP64 links only; its algorithm (mc_updates.h:7-64,109-115 and the PCC/PMC
  * masks of mc_updates_pcc.h / mc_updates_pmc.h) is kept step for step, with the
  * arithmetic in float except for the fix-ups done in double: the heat-bath
- * accept test, the length of the new link's spatial part, the Metropolis
- * action change and accept test, and the re-projection.
+ * accept test, the Metropolis action change and accept test, and the
+ * re-projection.
  *
  * The field holds float values (as doubles): links are read as floats and
  * written back as (double)float.  Draws come from Philox4x32-10 (Salmon,
@@ -708,9 +708,9 @@ static fquat staples32(const ora_lattice* h, int mu, int par, int id, const nbr_
   return A;
 }
 
-/* Kennedy-Pendleton (mc_updates.h:43-64) in float; the accept test
- * (1 - lf is within an ulp of 1 for a large coupling) and the length
- * n = 2 sqrt(lf (1 - lf)) of the spatial part in double */
+/* Kennedy-Pendleton (mc_updates.h:43-64) in float; the accept test in double
+ * (1 - lf is within an ulp of 1 for a large coupling); the length of the
+ * spatial part as n = 2 sqrt(lf (1 - lf)), free of cancellation */
 static fquat heat_bath32(fquat A, float beta, pstream* st, int* tries_out) {
   float det = f_det(A), rinv = 1.0f / sqrtf(det), a = det * rinv;
   A = f_scale(A, rinv);
@@ -724,9 +724,8 @@ static fquat heat_bath32(fquat A, float beta, pstream* st, int* tries_out) {
     if (!((double)aux * aux > 1.0 - (double)lf)) break;
   }
   *tries_out = tries;
-  double lfd = lf;
-  float x0 = (float)(1.0 - 2.0 * lfd);
-  float nrm = (float)(2.0 * sqrt(lfd * (1.0 - lfd)));
+  float x0 = 1.f - 2.f * lf;
+  float nrm = 2.f * sqrtf(lf * (1.f - lf));
   float ct = 2.f * ps_uniform(st) - 1.f;
   float ang = 6.2831853f * (ps_uniform(st) - 0.5f);
   float sp = sinf(ang), cp = cosf(ang);

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kBlock) batch_phase(BatchView B, BatchArgs a) 
   // FP32 draws: the replica's seed as key, its stream offset added to the
   // site index, the batch-wide drawing-phase counter (as for one lattice)
   PhaseArgs pa{R.beta, a.eps, a.upd, a.err, a.accept ? a.accept + R.site_off : nullptr, a.renorm,
-               R.seed, a.phase_ptr, a.phase_off, (unsigned int)R.stream_off};
+               R.seed, a.phase_ptr, a.phase_off, (unsigned int)R.stream_off, philox_keys(R.seed)};
   RngStore RS{B.rng + R.rng_off, R.g.vh};
   if (FP64) {
     Links64 L{B.lo + R.link_off, B.hi + R.link_off, R.g.vh};

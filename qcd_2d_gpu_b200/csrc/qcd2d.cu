@@ -165,7 +165,7 @@ Phase32Fn phase_fn32(int k, int bc, int kind) {
 // one pass over the six phases with one update kind; with `renorm` (FP32
 // only) every link is re-projected as it is stored
 int pass(qcd_lattice* h, int kind, int renorm = 0) {
-  PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, renorm, h->draw_key, h->draw_dev, 0, 0};
+  PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, renorm, h->draw_key, h->draw_dev, 0, 0, philox_keys(h->draw_key)};
   const dim3 grid(nblocks(h->g.slice), (unsigned int)h->g.lt);
   for (int k = 0; k < 6; k++) {
     a.phase_off = (unsigned int)k;
@@ -406,7 +406,7 @@ int launch_wave(qcd_lattice* h, const PassSpec* ps, int np, int stall_test = 0,
   CUDA_OR_FAIL(h, cudaMemsetAsync(h->wave_done, 0, (size_t)h->g.lt * sizeof(unsigned int), h->stream));
   CUDA_OR_FAIL(h, cudaMemsetAsync(h->wave_queue, 0, sizeof(unsigned int), h->stream));
   CUDA_OR_FAIL(h, cudaMemsetAsync(h->wave_abort, 0, sizeof(int), h->stream));
-  PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, 0, h->draw_key, h->draw_dev, 0, 0};
+  PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, 0, h->draw_key, h->draw_dev, 0, 0, philox_keys(h->draw_key)};
   const int sk = h->p.algo == QCD_ALGO_HEATBATH ? KIND_HB : KIND_METRO;
   const int bc = h->p.boundary;
   const unsigned int grid = (unsigned int)h->wave_grid;
@@ -484,7 +484,7 @@ int pairs_setup(qcd_lattice* h) {
 // writing the other one, which then becomes current.
 int pass_pairs(qcd_lattice* h, int kind, int renorm) {
   if (!h->q32alt || !h->sms) return fail(h, QCD_ERR_INVALID, "fused pairs used before their setup");
-  PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, renorm, h->draw_key, h->draw_dev, 0, 0};
+  PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, renorm, h->draw_key, h->draw_dev, 0, 0, philox_keys(h->draw_key)};
   const PairMaps& mc = h->pair_maps[h->q32 == h->pair_buf[0] ? 0 : 1];
   const PairMaps& ma = h->pair_maps[h->q32 == h->pair_buf[0] ? 1 : 0];
   CUDA_OR_FAIL(h, pair_pass32(h->q32, h->q32alt, mc, ma, h->g, h->p.boundary, kind, a, h->pair_seg, h->sms, h->stream));

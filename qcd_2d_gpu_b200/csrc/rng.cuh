@@ -91,17 +91,55 @@ struct Philox4x32 {
   }
 };
 
+// The ten round keys of a Philox4x32-10 key (the key bumped by the Weyl
+// increments before each round after the first): they depend on the seed
+// only, so a kernel receives them precomputed (in its parameters, read as
+// constant operands) instead of adding them again in every block.
+struct PhiloxKeys {
+  uint32_t k[20];  // round r: k[2r], k[2r + 1]
+};
+__host__ __device__ __forceinline__ PhiloxKeys philox_keys(unsigned long long seed) {
+  PhiloxKeys s;
+  uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  for (int r = 0; r < 10; r++) {
+    s.k[2 * r] = k0;
+    s.k[2 * r + 1] = k1;
+    k0 += Philox4x32::kW0;
+    k1 += Philox4x32::kW1;
+  }
+  return s;
+}
+// The same block as Philox4x32::block, with the round keys given.
+__host__ __device__ __forceinline__ void philox_block_rk(const uint32_t ctr[4], const PhiloxKeys& ks,
+                                                         uint32_t out[4]) {
+  uint32_t x0 = ctr[0], x1 = ctr[1], x2 = ctr[2], x3 = ctr[3];
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    const uint64_t p0 = (uint64_t)Philox4x32::kM0 * x0, p1 = (uint64_t)Philox4x32::kM1 * x2;
+    const uint32_t y0 = (uint32_t)(p1 >> 32) ^ x1 ^ ks.k[2 * r];
+    const uint32_t y2 = (uint32_t)(p0 >> 32) ^ x3 ^ ks.k[2 * r + 1];
+    x1 = (uint32_t)p1;
+    x3 = (uint32_t)p0;
+    x0 = y0;
+    x2 = y2;
+  }
+  out[0] = x0;
+  out[1] = x1;
+  out[2] = x2;
+  out[3] = x3;
+}
+
 // The draws of one link update: counter (site, block, phase lo, phase hi),
 // block = 0, 1, ... as the update consumes 32-bit words in order.  `phase`
 // numbers the drawing phases of the lattice (6 per heat-bath or Metropolis
 // pass), so no two updates share a counter.
 struct PhiloxStream {
-  uint32_t key[2], ctr[4];
+  const PhiloxKeys& ks;  // round keys of the key (the seed)
+  uint32_t ctr[4];
   uint32_t b0, b1, b2, b3;
   int left;
-  __device__ __forceinline__ PhiloxStream(unsigned long long seed, uint32_t site, unsigned long long phase) {
-    key[0] = (uint32_t)seed;
-    key[1] = (uint32_t)(seed >> 32);
+  __device__ __forceinline__ PhiloxStream(const PhiloxKeys& keys, uint32_t site, unsigned long long phase)
+      : ks(keys) {
     ctr[0] = site;
     ctr[1] = 0;
     ctr[2] = (uint32_t)phase;
@@ -111,7 +149,7 @@ struct PhiloxStream {
   __device__ __forceinline__ uint32_t next() {
     if (left == 0) {
       uint32_t o[4];
-      Philox4x32::block(ctr, key, o);
+      philox_block_rk(ctr, ks, o);
       ctr[1]++;
       b0 = o[0];
       b1 = o[1];

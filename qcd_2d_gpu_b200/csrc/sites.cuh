@@ -29,6 +29,7 @@ struct PhaseArgs {
   const unsigned long long* phase_ptr;
   unsigned int phase_off;
   unsigned int site_off;
+  PhiloxKeys keys;  // round keys of `seed` (philox_keys), set by whoever fills the arguments
 };
 
 // The drawing-phase counter of the FP32 draws lives on the device and is
@@ -95,10 +96,10 @@ __device__ __forceinline__ Quat<float> link_update32(const L& links, const Geo& 
   Quat<float> A = staple_sum<MU, BC, L, float>(links, g, n, PAR);
   Quat<float> U;
   if (KIND == KIND_HB) {
-    PhiloxStream st(a.seed, a.site_off + (unsigned int)gid, draw_phase(a));
+    PhiloxStream st(a.keys, a.site_off + (unsigned int)gid, draw_phase(a));
     U = heatbath_fast(A, a.beta, st, a.err);
   } else if (KIND == KIND_METRO) {
-    PhiloxStream st(a.seed, a.site_off + (unsigned int)gid, draw_phase(a));
+    PhiloxStream st(a.keys, a.site_off + (unsigned int)gid, draw_phase(a));
     U = links.ld_own(MU, PAR, n.id);
     int acc = metropolis_fast(U, A, a.beta, a.eps, a.upd, st);
     if (count_accept) atomicAdd(a.accept + PAR * g.vh + gid, acc);
@@ -116,10 +117,10 @@ __device__ __forceinline__ void site32(const Links32T<CG>& L, const RngStoreT<CG
   Quat<float> A = staple_sum<MU, BC, Links32T<CG>, float>(L, g, n, PAR);
   Quat<float> U;
   if (KIND == KIND_HB) {
-    PhiloxStream st(a.seed, a.site_off + (unsigned int)id, draw_phase(a));
+    PhiloxStream st(a.keys, a.site_off + (unsigned int)id, draw_phase(a));
     U = heatbath_fast(A, a.beta, st, a.err);
   } else if (KIND == KIND_METRO) {
-    PhiloxStream st(a.seed, a.site_off + (unsigned int)id, draw_phase(a));
+    PhiloxStream st(a.keys, a.site_off + (unsigned int)id, draw_phase(a));
     U = L.ld_own(MU, PAR, id);
     int acc = metropolis_fast(U, A, a.beta, a.eps, a.upd, st);
     add_accept<CG>(a.accept + PAR * g.vh + id, acc);

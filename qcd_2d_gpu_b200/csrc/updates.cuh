@@ -179,10 +179,10 @@ __device__ __forceinline__ Quat<double> overrelax_ref(Quat<double> A, const Quat
 // The FP32 updates draw from a generator G with uniform() (float in (0, 1])
 // and uniform_double() (double in (0, 1]): the counter-based PhiloxStream.
 
-// Kennedy-Pendleton in FP32.  The parts that lose accuracy in single precision
-// are done in double: the accept test (1 - lf is within an ulp of 1 for large
-// beta*|A|) and the length of the spatial part, n = 2 sqrt(lf (1 - lf)),
-// which replaces sqrt(1 - X0^2) and its cancellation as X0 -> 1.
+// Kennedy-Pendleton in FP32.  The accept test, which loses accuracy in single
+// precision (1 - lf is within an ulp of 1 for large beta*|A|), is done in
+// double.  The length of the spatial part is taken as n = 2 sqrt(lf (1 - lf))
+// instead of sqrt(1 - X0^2): no cancellation as X0 -> 1, so float suffices.
 template <class G>
 __device__ __forceinline__ Quat<float> heatbath_fast(Quat<float> A, float beta, G& st, int* err) {
   float det = q_det(A);
@@ -205,9 +205,8 @@ __device__ __forceinline__ Quat<float> heatbath_fast(Quat<float> A, float beta, 
       break;
     }
   }
-  double lfd = lf;
-  float x0 = (float)(1.0 - 2.0 * lfd);
-  float nrm = (float)(2.0 * sqrt(lfd * (1.0 - lfd)));
+  const float x0 = 1.f - 2.f * lf;
+  const float nrm = 2.f * sqrtf(lf * (1.f - lf));
   float ct = 2.f * st.uniform() - 1.f, sp, cp;
   __sincosf(6.2831853f * (st.uniform() - 0.5f), &sp, &cp);  // angle + pi
   float stt = sqrtf(fmaxf(0.f, 1.f - ct * ct));
