@@ -98,18 +98,24 @@ C4_SWEEPS = 200
 
 def c4_replicas():
     """96 replicas: Nt = Nx uniform over even 8..64, Ny over even 8..128, beta
-    uniform in [3, 12], boundary r mod 3, hot start for even r, seed 1234 + r
-    (numpy's PCG64 seeded with 1234 draws the shapes)."""
+    uniform in [3, 12], boundary r mod 3, hot start for even r (numpy's PCG64
+    seeded with 1234 draws the shapes).  Every replica has its own block of
+    MRG32k3a subsequences under the one seed 1234: replica r's streams are
+    curand_init(1234, offset_r + id, 0) with offset_r the half-sites of the
+    replicas before it, so no two streams of the batch coincide (the same
+    offsets separate the Philox site counters of the FP32 draws)."""
     import numpy as np
 
     rng = np.random.default_rng(1234)
     reps = []
+    offset = 0
     for r in range(96):
         lt = int(rng.choice(np.arange(8, 65, 2)))
         ly = int(rng.choice(np.arange(8, 129, 2)))
         beta = float(rng.uniform(3.0, 12.0))
-        reps.append(dict(lt=lt, lx=lt, ly=ly, beta=beta, boundary=r % 3, hot=int(r % 2 == 0), seed=1234 + r,
-                         stream_offset=0))
+        reps.append(dict(lt=lt, lx=lt, ly=ly, beta=beta, boundary=r % 3, hot=int(r % 2 == 0), seed=1234,
+                         stream_offset=offset))
+        offset += lt * lt * ly // 2
     return reps
 
 
@@ -414,7 +420,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-replica measurement")
     ap.add_argument("--lattice", type=int, nargs=3, default=None, help="override (testing only)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "accuracy", "c3-accuracy"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "accuracy", "c3-accuracy", "batch"])
     ap.add_argument("--schedule", default="auto", choices=["auto", "phases", "wavefront", "pairs"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
                     help="link precision of the timed workload (fp32 is the benchmark; fp64 for profiling)")
@@ -437,6 +443,14 @@ def main():
         import qcd_2d_gpu_b200 as q
 
         return accuracy_scan(args, q, torch)
+    if args.workload == "batch" and args.impl == "ours":
+        import torch
+
+        import qcd_2d_gpu_b200 as q
+
+        stream = torch.cuda.Stream()
+        print(json.dumps(run_batch_c4(q, torch, stream)))
+        return 0
     if args.workload == "c3-accuracy":
         import torch
 
