@@ -94,16 +94,28 @@ __global__ void __launch_bounds__(kBlock) batch_phase(BatchView B, BatchArgs a) 
   }
 }
 
-// curand_init(seed_r, stream_off_r + id, 0) per site of every replica, then
-// the replica's start (rand_init2 / rand_init2_pcc / id_init2 semantics)
+// curand_init(seed_r, stream_off_r + id, 0) per site of every replica (one
+// curand_init per CTA and a jump per thread, as rng_setup), then the
+// replica's start (rand_init2 / rand_init2_pcc / id_init2 semantics)
 template <bool FP64>
-__global__ void __launch_bounds__(kBlock) batch_setup(BatchView B) {
+__global__ void __launch_bounds__(kBlock) batch_setup(BatchView B, const uint32_t* __restrict__ jumps) {
   const int r = replica_of(B, blockIdx.x);
   const Replica& R = B.rep[r];
-  const int id = (blockIdx.x - R.cta_begin) * kBlock + threadIdx.x;
+  const int id0 = (blockIdx.x - R.cta_begin) * kBlock;
+  __shared__ unsigned int base[6];
+  if (threadIdx.x == 0) {
+    curandStateMRG32k3a_t s0;
+    curand_init(R.seed, (unsigned long long)(R.stream_off + id0), 0ull, &s0);
+    for (int i = 0; i < 3; i++) {
+      base[i] = s0.s1[i];
+      base[3 + i] = s0.s2[i];
+    }
+  }
+  __syncthreads();
+  const int id = id0 + threadIdx.x;
   if (id >= R.g.vh) return;
   curandStateMRG32k3a_t st;
-  curand_init(R.seed, (unsigned long long)(R.stream_off + id), 0ull, &st);
+  mrg_jump_from(base, jumps, threadIdx.x, &st);
   for (int p = 0; p < 2; p++) {
     const Nbr n = make_nbr(R.g, id, p);
     const bool frozen = R.bc == BC_PCC && at_y0(R.g, n);
@@ -250,6 +262,7 @@ struct qcd_batch {
   double2* lo = nullptr;
   double2* hi = nullptr;
   uint32_t* rng = nullptr;
+  uint32_t* mrg_jumps = nullptr;  // jump matrices that seed the streams (mrg_jump_table)
   unsigned long long* draw_dev = nullptr;  // drawing phases run so far (FP32 draws)
   int* accept = nullptr;
   int* err = nullptr;
@@ -353,6 +366,7 @@ void release(qcd_batch* b) {
   cudaFree(b->lo);
   cudaFree(b->hi);
   cudaFree(b->rng);
+  cudaFree(b->mrg_jumps);
   cudaFree(b->accept);
   cudaFree(b->err);
   cudaFree(b->draw_dev);
@@ -454,6 +468,10 @@ int qcd_batch_create(const qcd_replica* r, int n, const qcd_params* common, qcd_
     step(cudaMalloc(&b->q32, link_off * sizeof(float4)), "cudaMalloc(links)");
   }
   if (rc == QCD_OK) step(cudaMalloc(&b->rng, rng_off * sizeof(uint32_t)), "cudaMalloc(rng)");
+  if (rc == QCD_OK) step(cudaMalloc(&b->mrg_jumps, kMrgJumpWords * sizeof(uint32_t)), "cudaMalloc(jumps)");
+  if (rc == QCD_OK)
+    step(cudaMemcpy(b->mrg_jumps, mrg_jump_host(), kMrgJumpWords * sizeof(uint32_t), cudaMemcpyHostToDevice),
+         "jump table");
   if (rc == QCD_OK && common->algo == QCD_ALGO_METROPOLIS) {
     step(cudaMalloc(&b->accept, site_off * sizeof(int)), "cudaMalloc(accept)");
     if (rc == QCD_OK) step(cudaMemsetAsync(b->accept, 0, site_off * sizeof(int), b->stream), "memset");
@@ -503,9 +521,9 @@ int qcd_batch_set_stream(qcd_batch* b, void* stream) {
 int qcd_batch_init(qcd_batch* b) {
   if (!b) return QCD_ERR_INVALID;
   if (fp64(b))
-    batch_setup<true><<<b->ctas, kBlock, 0, b->stream>>>(view(b));
+    batch_setup<true><<<b->ctas, kBlock, 0, b->stream>>>(view(b), b->mrg_jumps);
   else
-    batch_setup<false><<<b->ctas, kBlock, 0, b->stream>>>(view(b));
+    batch_setup<false><<<b->ctas, kBlock, 0, b->stream>>>(view(b), b->mrg_jumps);
   BCUDA(b, cudaGetLastError());
   BCUDA(b, cudaMemsetAsync(b->cursor, 0, sizeof(int), b->stream));
   // a fresh start: the streams are re-seeded above, the counter of the FP32

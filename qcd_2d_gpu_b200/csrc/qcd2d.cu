@@ -31,8 +31,9 @@ struct qcd_lattice {
   float4* q32 = nullptr;     // FP32 store holding the current links
   float4* q32alt = nullptr;  // second FP32 store: the fused-pair schedule writes each pass's new links here
   size_t link_bytes = 0;
-  // MRG32k3a streams, 6 u32 planes
+  // MRG32k3a streams, 6 u32 planes, and the jump matrices that seed them
   uint32_t* rng = nullptr;
+  uint32_t* mrg_jumps = nullptr;
   // Metropolis accept counters (V ints) and analytic unit counts for HB/OR
   int* accept = nullptr;
   long long unit_passes = 0;  // HB/OR passes since the last reset
@@ -580,8 +581,13 @@ int run_passes(qcd_lattice* h, const PassSpec* ps, int np) {
 // late gives the same words as seeding at create.
 int ensure_rng(qcd_lattice* h) {
   if (h->rng) return QCD_OK;
+  if (!h->mrg_jumps) {
+    CUDA_OR_FAIL(h, cudaMalloc(&h->mrg_jumps, kMrgJumpWords * sizeof(uint32_t)));
+    CUDA_OR_FAIL(h, cudaMemcpyAsync(h->mrg_jumps, mrg_jump_host(), kMrgJumpWords * sizeof(uint32_t),
+                                    cudaMemcpyHostToDevice, h->stream));
+  }
   CUDA_OR_FAIL(h, cudaMalloc(&h->rng, 6 * (size_t)h->g.vh * sizeof(uint32_t)));
-  rng_setup<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(rngs(h), h->p.seed, h->g.vh);
+  rng_setup<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(rngs(h), h->p.seed, h->g.vh, h->mrg_jumps);
   LAUNCH_CHECK(h);
   return QCD_OK;
 }
@@ -592,6 +598,7 @@ void release(qcd_lattice* h) {
   cudaFree(h->q32);
   cudaFree(h->q32alt);
   cudaFree(h->rng);
+  cudaFree(h->mrg_jumps);
   cudaFree(h->accept);
   cudaFree(h->partials);
   cudaFree(h->counter);
@@ -685,11 +692,6 @@ int qcd_create(const qcd_params* p, qcd_lattice** out) {
     h->link_bytes = 6 * vh * sizeof(float4);
     if (rc == QCD_OK) step(cudaMalloc(&h->q32, 6 * vh * sizeof(float4)), "cudaMalloc(links)");
   }
-  // the FP64 sweep draws from the stored MRG32k3a streams at every update; an
-  // FP32 lattice needs them only for a hot start or a generator checkpoint,
-  // so it seeds them on first use (ensure_rng)
-  if (rc == QCD_OK && p->precision == QCD_PREC_FP64)
-    step(cudaMalloc(&h->rng, 6 * vh * sizeof(uint32_t)), "cudaMalloc(rng)");
   if (rc == QCD_OK && p->algo == QCD_ALGO_METROPOLIS) {
     step(cudaMalloc(&h->accept, 2 * vh * sizeof(int)), "cudaMalloc(accept)");
     if (rc == QCD_OK) step(cudaMemsetAsync(h->accept, 0, 2 * vh * sizeof(int), h->stream), "memset");
@@ -704,10 +706,10 @@ int qcd_create(const qcd_params* p, qcd_lattice** out) {
   if (rc == QCD_OK) step(cudaMallocHost(&h->result_host, 4 * sizeof(double)), "cudaMallocHost");
   if (rc == QCD_OK) step(cudaMemsetAsync(h->counter, 0, sizeof(unsigned int), h->stream), "memset");
   if (rc == QCD_OK) step(cudaMemsetAsync(h->err, 0, sizeof(int), h->stream), "memset");
-  if (rc == QCD_OK && h->rng) {
-    rng_setup<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(rngs(h), p->seed, h->g.vh);
-    step(cudaGetLastError(), "rng_setup");
-  }
+  // the FP64 sweep draws from the stored MRG32k3a streams at every update; an
+  // FP32 lattice needs them only for a hot start or a generator checkpoint,
+  // so it seeds them on first use
+  if (rc == QCD_OK && p->precision == QCD_PREC_FP64) rc = ensure_rng(h);
   if (rc == QCD_OK) step(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
   if (rc != QCD_OK) {
     fprintf(stderr, "qcd_create: %s\n", h->msg);

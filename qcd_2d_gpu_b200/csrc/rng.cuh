@@ -55,6 +55,100 @@ struct RngStoreT {
 };
 typedef RngStoreT<false> RngStore;
 
+// ------------------------------------------------- seeding many streams ----
+// curand_init(seed, id, 0) places stream id 2^127 steps after stream id - 1
+// (cuRAND's MRG32k3a subsequence length), and curand_init's skip-ahead walks
+// a table per set bit of id, so seeding millions of streams that way costs
+// tens of milliseconds.  The streams of a CTA are consecutive, so the CTA
+// seeds its first stream with curand_init and each thread j jumps from there
+// by J^j, J = A^(2^127), A the transition matrix of each MRG32k3a component
+// (L'Ecuyer, "Good parameters and implementations for combined multiple
+// recursive random number generators", Operations Research 47(1), 1999:
+// x_n = 1403580 x_{n-2} - 810728 x_{n-3} mod m1,
+// y_n = 527612 y_{n-1} - 1370589 y_{n-3} mod m2, state (s[0], s[1], s[2]) =
+// oldest to newest).  The matrices J^0 .. J^255 are computed on the host by
+// repeated squaring.  The states equal curand_init's word for word (the FP64
+// path's bit-for-bit tests against the reference depend on it).
+constexpr uint64_t kMrgM1 = 4294967087ull, kMrgM2 = 4294944443ull;
+constexpr int kMrgJumps = 256;  // one matrix per thread of a CTA
+constexpr int kMrgJumpWords = kMrgJumps * 18;  // J^j: component 1 then 2, 3x3 row-major
+
+inline void mrg_jump_table(uint32_t* out) {
+  typedef unsigned __int128 u128;
+  struct M3 {
+    uint64_t a[9];
+  };
+  auto mul = [](const M3& x, const M3& y, uint64_t m) {
+    M3 r;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) {
+        u128 s = 0;
+        for (int k = 0; k < 3; k++) s += (u128)x.a[3 * i + k] * y.a[3 * k + j];
+        r.a[3 * i + j] = (uint64_t)(s % m);
+      }
+    return r;
+  };
+  M3 a1 = {{0, 1, 0, 0, 0, 1, kMrgM1 - 810728, 1403580, 0}};
+  M3 a2 = {{0, 1, 0, 0, 0, 1, kMrgM2 - 1370589, 0, 527612}};
+  for (int i = 0; i < 127; i++) {  // A^(2^127)
+    a1 = mul(a1, a1, kMrgM1);
+    a2 = mul(a2, a2, kMrgM2);
+  }
+  M3 p1 = {{1, 0, 0, 0, 1, 0, 0, 0, 1}}, p2 = p1;
+  for (int j = 0; j < kMrgJumps; j++) {
+    for (int k = 0; k < 9; k++) {
+      out[18 * j + k] = (uint32_t)p1.a[k];
+      out[18 * j + 9 + k] = (uint32_t)p2.a[k];
+    }
+    p1 = mul(p1, a1, kMrgM1);
+    p2 = mul(p2, a2, kMrgM2);
+  }
+}
+
+// The table on the host, built once per process.
+inline const uint32_t* mrg_jump_host() {
+  struct T {
+    uint32_t w[kMrgJumpWords];
+    T() { mrg_jump_table(w); }
+  };
+  static const T t;
+  return t.w;
+}
+
+// s <- M s mod m for one component (M: 9 words, row-major)
+__device__ __forceinline__ void mrg_mat_vec(const uint32_t* __restrict__ M, unsigned int s[3], uint64_t m) {
+  uint64_t r[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    uint64_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      acc += ((uint64_t)__ldg(M + 3 * i + k) * s[k]) % m;  // each term < m < 2^32: no overflow
+    }
+    r[i] = acc % m;
+  }
+  s[0] = (unsigned int)r[0];
+  s[1] = (unsigned int)r[1];
+  s[2] = (unsigned int)r[2];
+}
+
+// The state of stream (first stream of the CTA) + j: the CTA's thread 0 has
+// put curand_init's state of its first stream in base[6] (s1 then s2).
+__device__ __forceinline__ void mrg_jump_from(const unsigned int base[6], const uint32_t* table, int j,
+                                              curandStateMRG32k3a_t* st) {
+  unsigned int s1[3] = {base[0], base[1], base[2]}, s2[3] = {base[3], base[4], base[5]};
+  mrg_mat_vec(table + 18 * j, s1, kMrgM1);
+  mrg_mat_vec(table + 18 * j + 9, s2, kMrgM2);
+  for (int i = 0; i < 3; i++) {
+    st->s1[i] = s1[i];
+    st->s2[i] = s2[i];
+  }
+  st->boxmuller_flag = 0;
+  st->boxmuller_flag_double = 0;
+  st->boxmuller_extra = 0.f;
+  st->boxmuller_extra_double = 0.0;
+}
+
 // ------------------------------------------------ counter-based stream ----
 // Philox4x32-10 (J. K. Salmon, M. A. Moraes, R. O. Dror, D. E. Shaw,
 // "Parallel random numbers: as easy as 1, 2, 3", SC'11): a 4 x 32-bit counter

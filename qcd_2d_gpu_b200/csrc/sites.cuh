@@ -237,27 +237,30 @@ __host__ __device__ __forceinline__ unsigned int measure_blocks(long long vh) {
   return (unsigned int)(nb < kMeasureMaxBlocks ? nb : kMeasureMaxBlocks);
 }
 
-// Energy and plaquette sums of the sites id = c*256 + tid, + nb*256, ... of
-// CTA c of nb (both parities): -(1 - P_xt) and 3 - sum of the three 1 - P.
-// A multiply-high finds the site's t-slice; the neighbours come from the
-// slice position (multiply-high).
+// Energy and plaquette sums of the items k = c*256 + tid, + nb*256, ... of
+// CTA c of nb, item k < V being the site of sublattice p = k / (V/2) with
+// sublattice index k - p V/2: -(1 - P_xt) and 3 - the sum of the three 1 - P.
+// One site of one parity per item keeps few links live per thread.  A
+// multiply-high finds the site's t-slice; the neighbours come from the slice
+// position (multiply-high).
 template <class L, bool PMC>
 __device__ __forceinline__ void measure_sites(const L& links, const Geo& g, int c, int nb, double& e, double& pl) {
-  for (int id = c * kBlock + threadIdx.x; id < g.vh; id += nb * kBlock) {
+  const unsigned int items = 2u * (unsigned int)g.vh;
+  for (unsigned int k = (unsigned int)c * kBlock + threadIdx.x; k < items; k += (unsigned int)nb * kBlock) {
+    const int p = k >= (unsigned int)g.vh;
+    const int id = (int)k - p * g.vh;
     const int t = div_by((unsigned int)id, g.slice_m);
     const int s = id - t * g.slice;
-    for (int p = 0; p < 2; p++) {
-      const Nbr n = make_nbr_slice(g, s, t, p);
-      double a = plaq(links, DIR_Y, DIR_X, p, id, n.yp, n.xp);
-      double b = plaq(links, DIR_Y, DIR_T, p, id, n.yp, n.tp);
-      double cc = plaq(links, DIR_X, DIR_T, p, id, n.xp, n.tp);
-      if (PMC && at_ytop(g, n)) {
-        a = 0;
-        b = 0;
-      }
-      e += -cc;
-      pl += 3 - a - b - cc;  // the 1/3 of the plaquette average is applied once per thread
+    const Nbr n = make_nbr_slice(g, s, t, p);
+    double a = plaq(links, DIR_Y, DIR_X, p, id, n.yp, n.xp);
+    double b = plaq(links, DIR_Y, DIR_T, p, id, n.yp, n.tp);
+    double cc = plaq(links, DIR_X, DIR_T, p, id, n.xp, n.tp);
+    if (PMC && at_ytop(g, n)) {
+      a = 0;
+      b = 0;
     }
+    e += -cc;
+    pl += 3 - a - b - cc;  // the 1/3 of the plaquette average is applied once per thread
   }
 }
 
