@@ -259,7 +259,8 @@ typedef struct qcd_replica {
   int boundary;            /* enum qcd_boundary */
   int hot;                 /* 1: hot start (rand_init2 / rand_init2_pcc), 0: cold */
   unsigned long long seed;
-  long long stream_offset; /* first MRG32k3a subsequence / Philox site counter of this replica */
+  long long stream_offset; /* first MRG32k3a subsequence / Philox site counter of this replica
+                              (stream_offset + V/2 <= 2^40) */
 } qcd_replica;
 typedef struct qcd_batch qcd_batch;
 

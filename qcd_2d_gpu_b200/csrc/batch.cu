@@ -103,14 +103,7 @@ __global__ void __launch_bounds__(kBlock) batch_setup(BatchView B, const uint32_
   const Replica& R = B.rep[r];
   const int id0 = (blockIdx.x - R.cta_begin) * kBlock;
   __shared__ unsigned int base[6];
-  if (threadIdx.x == 0) {
-    curandStateMRG32k3a_t s0;
-    curand_init(R.seed, (unsigned long long)(R.stream_off + id0), 0ull, &s0);
-    for (int i = 0; i < 3; i++) {
-      base[i] = s0.s1[i];
-      base[3 + i] = s0.s2[i];
-    }
-  }
+  if (threadIdx.x == 0) mrg_cta_base(base, jumps, R.seed, (unsigned long long)(R.stream_off + id0));
   __syncthreads();
   const int id = id0 + threadIdx.x;
   if (id >= R.g.vh) return;
@@ -398,7 +391,8 @@ int qcd_batch_create(const qcd_replica* r, int n, const qcd_params* common, qcd_
   for (int i = 0; i < n; i++) {
     const qcd_replica& x = r[i];
     if (x.lt < 2 || x.lx < 2 || x.ly < 2 || (x.lt & 1) || (x.lx & 1) || (x.ly & 1) || !(x.beta > 0.f) ||
-        x.boundary < 0 || x.boundary > 2 || x.stream_offset < 0) {
+        x.boundary < 0 || x.boundary > 2 || x.stream_offset < 0 ||
+        x.stream_offset > kMrgMaxStreams - (long long)x.lt * x.lx * x.ly / 2) {
       delete b;
       return QCD_ERR_INVALID;
     }

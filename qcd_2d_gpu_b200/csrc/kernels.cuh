@@ -29,22 +29,15 @@ __global__ void __launch_bounds__(kBlock) phase32(Links32 L, RngStore R, Geo g, 
 }
 
 // ------------------------------------------------------------ RNG setup --
-// curand_init(seed, id, 0) per half-lattice site (lattice_setup.h:15-21): one
-// curand_init per CTA, for its first site, and a jump of j subsequences for
-// the CTA's thread j (mrg_jump_from; `jumps` holds mrg_jump_table).
+// curand_init(seed, id, 0) per half-lattice site (lattice_setup.h:15-21),
+// by jumps from curand_init(seed, 0, 0) (mrg_cta_base, mrg_jump_from;
+// `jumps` holds mrg_jump_table).
 static_assert(kBlock == kMrgJumps, "one jump matrix per thread of a CTA");
 __global__ void __launch_bounds__(kBlock) rng_setup(RngStore R, unsigned long long seed, int vh,
                                                     const uint32_t* __restrict__ jumps) {
   __shared__ unsigned int base[6];
   const int id0 = blockIdx.x * kBlock;
-  if (threadIdx.x == 0) {
-    curandStateMRG32k3a_t st;
-    curand_init(seed, (unsigned long long)id0, 0ull, &st);
-    for (int i = 0; i < 3; i++) {
-      base[i] = st.s1[i];
-      base[3 + i] = st.s2[i];
-    }
-  }
+  if (threadIdx.x == 0) mrg_cta_base(base, jumps, seed, (unsigned long long)id0);
   __syncthreads();
   const int id = id0 + threadIdx.x;
   if (id >= vh) return;

@@ -56,22 +56,28 @@ struct RngStoreT {
 typedef RngStoreT<false> RngStore;
 
 // ------------------------------------------------- seeding many streams ----
-// curand_init(seed, id, 0) places stream id 2^127 steps after stream id - 1
-// (cuRAND's MRG32k3a subsequence length), and curand_init's skip-ahead walks
-// a table per set bit of id, so seeding millions of streams that way costs
-// tens of milliseconds.  The streams of a CTA are consecutive, so the CTA
-// seeds its first stream with curand_init and each thread j jumps from there
-// by J^j, J = A^(2^127), A the transition matrix of each MRG32k3a component
+// curand_init(seed, id, 0) places stream id 2^76 steps after stream id - 1
+// (it truncates the subsequence to 51 bits to stay inside one 2^127-step
+// sequence: L'Ecuyer's substreams).  Its skip-ahead costs about a millisecond
+// per call for the ids of a large lattice, so the streams are seeded here
+// from curand_init(seed, 0, 0) alone: stream id is J^id applied to it, with J
+// = A^(2^76) and A the transition matrix of each MRG32k3a component
 // (L'Ecuyer, "Good parameters and implementations for combined multiple
 // recursive random number generators", Operations Research 47(1), 1999:
 // x_n = 1403580 x_{n-2} - 810728 x_{n-3} mod m1,
 // y_n = 527612 y_{n-1} - 1370589 y_{n-3} mod m2, state (s[0], s[1], s[2]) =
-// oldest to newest).  The matrices J^0 .. J^255 are computed on the host by
-// repeated squaring.  The states equal curand_init's word for word (the FP64
-// path's bit-for-bit tests against the reference depend on it).
+// oldest to newest).  id is taken in base-256 digits, J^id = prod_k
+// (J^(256^k))^(d_k), from tables of J^(j 256^k), j < 256, k < 5 (ids below
+// 2^40) built on the host by repeated squaring.  Thread 0 of a CTA jumps to the
+// CTA's first stream, every thread on by its index.  The states equal
+// curand_init's word for word (the FP64 path's bit-for-bit tests against the
+// reference depend on it).
 constexpr uint64_t kMrgM1 = 4294967087ull, kMrgM2 = 4294944443ull;
-constexpr int kMrgJumps = 256;  // one matrix per thread of a CTA
-constexpr int kMrgJumpWords = kMrgJumps * 18;  // J^j: component 1 then 2, 3x3 row-major
+constexpr int kMrgSubseqLog2 = 76;  // steps between consecutive subsequences: 2^76
+constexpr int kMrgDigits = 5;       // base-256 digits of a stream number: ids < 2^40
+constexpr int kMrgJumps = 256;
+constexpr int kMrgJumpWords = kMrgDigits * kMrgJumps * 18;  // [digit][j]: component 1 then 2, 3x3 row-major
+constexpr long long kMrgMaxStreams = 1ll << 40;
 
 inline void mrg_jump_table(uint32_t* out) {
   typedef unsigned __int128 u128;
@@ -90,18 +96,23 @@ inline void mrg_jump_table(uint32_t* out) {
   };
   M3 a1 = {{0, 1, 0, 0, 0, 1, kMrgM1 - 810728, 1403580, 0}};
   M3 a2 = {{0, 1, 0, 0, 0, 1, kMrgM2 - 1370589, 0, 527612}};
-  for (int i = 0; i < 127; i++) {  // A^(2^127)
+  for (int i = 0; i < kMrgSubseqLog2; i++) {  // J = A^(2^76)
     a1 = mul(a1, a1, kMrgM1);
     a2 = mul(a2, a2, kMrgM2);
   }
-  M3 p1 = {{1, 0, 0, 0, 1, 0, 0, 0, 1}}, p2 = p1;
-  for (int j = 0; j < kMrgJumps; j++) {
-    for (int k = 0; k < 9; k++) {
-      out[18 * j + k] = (uint32_t)p1.a[k];
-      out[18 * j + 9 + k] = (uint32_t)p2.a[k];
+  for (int d = 0; d < kMrgDigits; d++) {  // a = J^(256^d)
+    M3 p1 = {{1, 0, 0, 0, 1, 0, 0, 0, 1}}, p2 = p1;
+    for (int j = 0; j < kMrgJumps; j++) {
+      uint32_t* o = out + ((size_t)d * kMrgJumps + j) * 18;
+      for (int k = 0; k < 9; k++) {
+        o[k] = (uint32_t)p1.a[k];
+        o[9 + k] = (uint32_t)p2.a[k];
+      }
+      p1 = mul(p1, a1, kMrgM1);
+      p2 = mul(p2, a2, kMrgM2);
     }
-    p1 = mul(p1, a1, kMrgM1);
-    p2 = mul(p2, a2, kMrgM2);
+    a1 = p1;  // J^(256^(d+1))
+    a2 = p2;
   }
 }
 
@@ -122,9 +133,7 @@ __device__ __forceinline__ void mrg_mat_vec(const uint32_t* __restrict__ M, unsi
   for (int i = 0; i < 3; i++) {
     uint64_t acc = 0;
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-      acc += ((uint64_t)__ldg(M + 3 * i + k) * s[k]) % m;  // each term < m < 2^32: no overflow
-    }
+    for (int k = 0; k < 3; k++) acc += ((uint64_t)__ldg(M + 3 * i + k) * s[k]) % m;  // terms < m < 2^32
     r[i] = acc % m;
   }
   s[0] = (unsigned int)r[0];
@@ -132,16 +141,42 @@ __device__ __forceinline__ void mrg_mat_vec(const uint32_t* __restrict__ M, unsi
   s[2] = (unsigned int)r[2];
 }
 
-// The state of stream (first stream of the CTA) + j: the CTA's thread 0 has
-// put curand_init's state of its first stream in base[6] (s1 then s2).
+// s (s1 then s2) <- J^id s for 0 <= id < 2^40, from digit `first_digit` on
+__device__ __forceinline__ void mrg_jump(unsigned int s[6], const uint32_t* table, unsigned long long id,
+                                        int first_digit = 0) {
+  id >>= 8 * first_digit;
+  for (int d = first_digit; d < kMrgDigits && id; d++, id >>= 8) {
+    const int j = (int)(id & 255u);
+    if (!j) continue;
+    const uint32_t* M = table + ((size_t)d * kMrgJumps + j) * 18;
+    mrg_mat_vec(M, s, kMrgM1);
+    mrg_mat_vec(M + 9, s + 3, kMrgM2);
+  }
+}
+
+// The CTA's thread 0 puts the state of stream `first` (curand_init(seed,
+// first, 0)) in base[6]; the CTA then reads it with mrg_jump_from.
+__device__ __forceinline__ void mrg_cta_base(unsigned int base[6], const uint32_t* table, unsigned long long seed,
+                                             unsigned long long first) {
+  curandStateMRG32k3a_t s0;
+  curand_init(seed, 0ull, 0ull, &s0);
+  unsigned int s[6] = {s0.s1[0], s0.s1[1], s0.s1[2], s0.s2[0], s0.s2[1], s0.s2[2]};
+  mrg_jump(s, table, first);
+  for (int i = 0; i < 6; i++) base[i] = s[i];
+}
+
+// The state of stream (the CTA's first stream) + j, 0 <= j < 256.
 __device__ __forceinline__ void mrg_jump_from(const unsigned int base[6], const uint32_t* table, int j,
                                               curandStateMRG32k3a_t* st) {
-  unsigned int s1[3] = {base[0], base[1], base[2]}, s2[3] = {base[3], base[4], base[5]};
-  mrg_mat_vec(table + 18 * j, s1, kMrgM1);
-  mrg_mat_vec(table + 18 * j + 9, s2, kMrgM2);
+  unsigned int s[6] = {base[0], base[1], base[2], base[3], base[4], base[5]};
+  if (j) {
+    const uint32_t* M = table + (size_t)j * 18;
+    mrg_mat_vec(M, s, kMrgM1);
+    mrg_mat_vec(M + 9, s + 3, kMrgM2);
+  }
   for (int i = 0; i < 3; i++) {
-    st->s1[i] = s1[i];
-    st->s2[i] = s2[i];
+    st->s1[i] = s[i];
+    st->s2[i] = s[3 + i];
   }
   st->boxmuller_flag = 0;
   st->boxmuller_flag_double = 0;
@@ -258,8 +293,15 @@ struct PhiloxStream {
     left--;
     return v;
   }
-  // (k + 1) / 2^24 for the top 24 bits k: exact floats in (0, 1]
-  __device__ __forceinline__ float uniform() { return (float)((next() >> 8) + 1u) * 5.9604644775390625e-8f; }
+  // The next whole block of four words (for a consumer whose draws come in
+  // fours; a stream is read either this way or word by word, not both).
+  __device__ __forceinline__ void block(uint32_t o[4]) {
+    philox_block_rk(ctr, ks, o);
+    ctr[1]++;
+  }
+  // (k + 1) / 2^24 for the top 24 bits k of a word: exact floats in (0, 1]
+  __device__ __forceinline__ static float u24(uint32_t w) { return (float)((w >> 8) + 1u) * 5.9604644775390625e-8f; }
+  __device__ __forceinline__ float uniform() { return u24(next()); }
   // (k + 1) / 2^53 from 53 bits of two words: exact doubles in (0, 1]
   __device__ __forceinline__ double uniform_double() {
     const uint64_t hi = next(), lo = next();

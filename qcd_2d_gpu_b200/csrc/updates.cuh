@@ -183,6 +183,10 @@ __device__ __forceinline__ Quat<double> overrelax_ref(Quat<double> A, const Quat
 // precision (1 - lf is within an ulp of 1 for large beta*|A|), is done in
 // double.  The length of the spatial part is taken as n = 2 sqrt(lf (1 - lf))
 // instead of sqrt(1 - X0^2): no cancellation as X0 -> 1, so float suffices.
+// The draws come from the counter-based stream a whole block at a time: each
+// try of the rejection loop takes one block (r0, r1, r2 and the accept
+// uniform), the direction the first two words of the next one, the same
+// words in the same order as drawing them one by one.
 template <class G>
 __device__ __forceinline__ Quat<float> heatbath_fast(Quat<float> A, float beta, G& st, int* err) {
   float det = q_det(A);
@@ -191,14 +195,15 @@ __device__ __forceinline__ Quat<float> heatbath_fast(Quat<float> A, float beta, 
   A = Quat<float>{A.w * rinv, A.x * rinv, A.y * rinv, A.z * rinv};
   float inv = 0.5f / (a * beta);
   float lf;
-  float aux;
+  uint32_t w[4];
   for (int tries = 1;; tries++) {
-    float r0 = st.uniform(), r1 = st.uniform(), r2 = st.uniform();
+    st.block(w);
+    const float r0 = G::u24(w[0]), r1 = G::u24(w[1]), r2 = G::u24(w[2]);
     // hardware approximations (absolute error ~2^-21): cos(2 pi r1) evaluated
     // as -cos(2 pi (r1 - 1/2)) keeps the argument in [-pi, pi]
     float c = -__cosf(6.2831853f * (r1 - 0.5f));
     lf = -(__logf(r0) + c * c * __logf(r2)) * inv;
-    aux = 1.f - st.uniform();
+    const float aux = 1.f - G::u24(w[3]);
     if (!((double)aux * aux > 1.0 - (double)lf)) break;
     if (tries >= QCD_HB_MAX_TRIES) {
       atomicOr(err, DEVERR_HB_LOOP);
@@ -207,8 +212,9 @@ __device__ __forceinline__ Quat<float> heatbath_fast(Quat<float> A, float beta, 
   }
   const float x0 = 1.f - 2.f * lf;
   const float nrm = 2.f * sqrtf(lf * (1.f - lf));
-  float ct = 2.f * st.uniform() - 1.f, sp, cp;
-  __sincosf(6.2831853f * (st.uniform() - 0.5f), &sp, &cp);  // angle + pi
+  st.block(w);
+  float ct = 2.f * G::u24(w[0]) - 1.f, sp, cp;
+  __sincosf(6.2831853f * (G::u24(w[1]) - 0.5f), &sp, &cp);  // angle + pi
   float stt = sqrtf(fmaxf(0.f, 1.f - ct * ct));
   Quat<float> X{x0, nrm * ct, -nrm * stt * cp, -nrm * stt * sp};
   return q_mul_bd(X, A);
