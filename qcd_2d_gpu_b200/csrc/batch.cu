@@ -66,7 +66,7 @@ struct BatchArgs {
 };
 
 template <int MU, int PAR, int KIND, bool FP64>
-__global__ void __launch_bounds__(kBlock) batch_phase(BatchView B, BatchArgs a) {
+__global__ void __launch_bounds__(kBlock, 6) batch_phase(BatchView B, BatchArgs a) {
   const int r = replica_of(B, blockIdx.x);
   const Replica& R = B.rep[r];
   const int id = (blockIdx.x - R.cta_begin) * kBlock + threadIdx.x;

@@ -227,13 +227,16 @@ __device__ __forceinline__ double plaq(const L& links, int mu, int nu, int p, in
   return 1 - A.w;
 }
 
-// CTAs of a measurement: one per 256 sites up to a fixed cap, the threads
-// striding over the sites, so a large lattice makes a few thousand partial
-// sums (added by the last CTA).  The count depends on the lattice only, so
-// the summation order is the same on every device.
+// CTAs of a measurement: one per 1024 half-lattice sites (each thread then
+// sums at least four sites of each parity, which amortises the CTA's
+// reduction) up to a fixed cap, the threads striding over the sites, so a
+// large lattice makes a few thousand partial sums (added by the last CTA).
+// The count depends on the lattice only, so the summation order is the same
+// on every device and for a lattice measured alone or in a batch.
 constexpr long long kMeasureMaxBlocks = 4096;
+constexpr long long kMeasureSitesPerBlock = 4 * kBlock;
 __host__ __device__ __forceinline__ unsigned int measure_blocks(long long vh) {
-  const long long nb = (vh + kBlock - 1) / kBlock;
+  const long long nb = (vh + kMeasureSitesPerBlock - 1) / kMeasureSitesPerBlock;
   return (unsigned int)(nb < kMeasureMaxBlocks ? nb : kMeasureMaxBlocks);
 }
 
