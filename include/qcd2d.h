@@ -246,7 +246,7 @@ const char* qcd_status_string(int status);
  * whole batch is the six phase launches of one lattice, each covering every
  * replica, and a measurement is one launch writing every replica's
  * (energy, plaquette).  qcd_batch_run captures one measurement interval as a
- * CUDA graph and replays it.  Replica r starts (and, in FP64, draws) from
+ * CUDA graph (per group of replicas, see qcd_batch_set_groups) and replays it.  Replica r starts (and, in FP64, draws) from
  * MRG32k3a streams curand_init(seed_r, stream_offset_r + id, 0); its FP32
  * sweep draws from the Philox counters of site stream_offset_r + id under key
  * seed_r.  With stream_offset 0 a replica reproduces a single lattice of the
@@ -276,6 +276,22 @@ int qcd_batch_reserve(qcd_batch* b, int capacity);
 /* `sweeps` sweeps of every replica, measuring after every `measure_every`
    sweeps (0: never); with use_graph the interval runs as a CUDA graph */
 int qcd_batch_run(qcd_batch* b, int sweeps, int measure_every, int use_graph);
+/* Groups: the replicas are swept in groups of consecutive replicas holding
+   at most bytes_per_group bytes of links (at least one replica each; 0: one
+   group of everything; default 64 MB), each group going through all the
+   sweeps of a qcd_batch_run while its links stay in L2 before the next group
+   starts.  Replicas are independent and every group keeps its own
+   drawing-phase counter and measurement cursor, so the results do not depend
+   on the grouping. */
+int qcd_batch_set_groups(qcd_batch* b, long long bytes_per_group);
+/* number of groups */
+int qcd_batch_groups(const qcd_batch* b);
+/* Autotuner of the grouping: times sweeps_per_trial sweeps (0: 20; with a
+   measurement after each when a series is reserved, as CUDA graphs) for one
+   group of everything and groups of 128 to 16 MB of links, restores the
+   batch's links, streams, counters, cursors and series exactly, and keeps the
+   fastest grouping (its bytes and ms per sweep, when the pointers are not NULL). */
+int qcd_batch_autotune(qcd_batch* b, int sweeps_per_trial, long long* bytes_out, double* ms_per_sweep_out);
 /* wait for the batch's stream; reports device-side errors */
 int qcd_batch_synchronize(qcd_batch* b);
 /* measurements taken so far (per replica) */

@@ -170,6 +170,9 @@ _SIGS = {
     "qcd_batch_reserve": (_I, [_P, _I]),
     "qcd_batch_run": (_I, [_P, _I, _I, _I]),
     "qcd_batch_synchronize": (_I, [_P]),
+    "qcd_batch_set_groups": (_I, [_P, ctypes.c_longlong]),
+    "qcd_batch_groups": (_I, [_P]),
+    "qcd_batch_autotune": (_I, [_P, _I, ctypes.POINTER(ctypes.c_longlong), _DP]),
     "qcd_batch_measured": (_I, [_P]),
     "qcd_batch_series": (_I, [_P, _I, _P, _P, _I]),
     "qcd_batch_store_config": (_I, [_P, _I, _P]),
@@ -444,6 +447,20 @@ class Batch:
 
     def synchronize(self):
         self._check(self._lib.qcd_batch_synchronize(self._h), "synchronize")
+
+    def set_groups(self, bytes_per_group):
+        """Sweep the replicas in groups of at most this many bytes of links (0: one group)."""
+        self._check(self._lib.qcd_batch_set_groups(self._h, int(bytes_per_group)), "set_groups")
+
+    def groups(self):
+        return self._lib.qcd_batch_groups(self._h)
+
+    def autotune(self, sweeps_per_trial=0):
+        """Pick the fastest grouping (the batch's state is preserved)."""
+        nb, ms = ctypes.c_longlong(), ctypes.c_double()
+        self._check(self._lib.qcd_batch_autotune(self._h, sweeps_per_trial, ctypes.byref(nb), ctypes.byref(ms)),
+                    "autotune")
+        return {"bytes_per_group": nb.value, "groups": self.groups(), "ms_per_sweep": ms.value}
 
     def measured(self):
         k = self._lib.qcd_batch_measured(self._h)

@@ -46,13 +46,16 @@ struct BatchView {
   const Replica* rep;
   const int* cta_rep;  // replica of every CTA of a batched launch
   const int* mcta_rep; // replica of every CTA of a batched measurement
-  int n;
+  int n;               // replicas the launch covers
+  int cta0, mcta0;     // first CTA of the launch in the batch's CTA tables (a group's offset)
   float4* q32;
   double2* lo;
   double2* hi;
   uint32_t* rng;
 };
 
+// a launch's CTA in the batch's CTA table, and its replica
+__device__ __forceinline__ int batch_cta(const BatchView& B) { return (int)blockIdx.x + B.cta0; }
 __device__ __forceinline__ int replica_of(const BatchView& B, int cta) { return __ldg(B.cta_rep + cta); }
 
 struct BatchArgs {
@@ -67,9 +70,10 @@ struct BatchArgs {
 
 template <int MU, int PAR, int KIND, bool FP64>
 __global__ void __launch_bounds__(kBlock, 6) batch_phase(BatchView B, BatchArgs a) {
-  const int r = replica_of(B, blockIdx.x);
+  const int cta = batch_cta(B);
+  const int r = replica_of(B, cta);
   const Replica& R = B.rep[r];
-  const int id = (blockIdx.x - R.cta_begin) * kBlock + threadIdx.x;
+  const int id = (cta - R.cta_begin) * kBlock + threadIdx.x;
   if (id >= R.g.vh) return;
   const Nbr n = make_nbr_fast(R.g, id, PAR);
   // FP32 draws: the replica's seed as key, its stream offset added to the
@@ -99,9 +103,10 @@ __global__ void __launch_bounds__(kBlock, 6) batch_phase(BatchView B, BatchArgs 
 // replica's start (rand_init2 / rand_init2_pcc / id_init2 semantics)
 template <bool FP64>
 __global__ void __launch_bounds__(kBlock) batch_setup(BatchView B, const uint32_t* __restrict__ jumps) {
-  const int r = replica_of(B, blockIdx.x);
+  const int cta = batch_cta(B);
+  const int r = replica_of(B, cta);
   const Replica& R = B.rep[r];
-  const int id0 = (blockIdx.x - R.cta_begin) * kBlock;
+  const int id0 = (cta - R.cta_begin) * kBlock;
   __shared__ unsigned int base[6];
   if (threadIdx.x == 0) mrg_cta_base(base, jumps, R.seed, (unsigned long long)(R.stream_off + id0));
   __syncthreads();
@@ -136,9 +141,10 @@ __global__ void __launch_bounds__(kBlock) batch_setup(BatchView B, const uint32_
 
 template <bool FP64>
 __global__ void __launch_bounds__(kBlock) batch_normalize(BatchView B) {
-  const int r = replica_of(B, blockIdx.x);
+  const int cta = batch_cta(B);
+  const int r = replica_of(B, cta);
   const Replica& R = B.rep[r];
-  const int id = (blockIdx.x - R.cta_begin) * kBlock + threadIdx.x;
+  const int id = (cta - R.cta_begin) * kBlock + threadIdx.x;
   if (id >= R.g.vh) return;
   for (int p = 0; p < 2; p++)
     for (int d = 0; d < 3; d++) {
@@ -163,7 +169,8 @@ template <bool FP64>
 __global__ void __launch_bounds__(kBlock) batch_measure(BatchView B, double2* partials, unsigned int* rep_count,
                                                         unsigned int* all_count, int* cursor, double2* series,
                                                         int cap) {
-  const int r = __ldg(B.mcta_rep + blockIdx.x);
+  const int mcta = (int)blockIdx.x + B.mcta0;  // CTA in the batch's measurement table
+  const int r = __ldg(B.mcta_rep + mcta);
   const Replica& R = B.rep[r];
   const int nblk = (int)measure_blocks(R.g.vh);
   const int k = *(volatile int*)cursor;  // advanced only by the last CTA below
@@ -171,21 +178,21 @@ __global__ void __launch_bounds__(kBlock) batch_measure(BatchView B, double2* pa
   if (FP64) {
     Links64 L{B.lo + R.link_off, B.hi + R.link_off, R.g.vh};
     if (R.bc == BC_PMC)
-      measure_sites<Links64, true>(L, R.g, blockIdx.x - R.mcta_begin, nblk, e, pl);
+      measure_sites<Links64, true>(L, R.g, mcta - R.mcta_begin, nblk, e, pl);
     else
-      measure_sites<Links64, false>(L, R.g, blockIdx.x - R.mcta_begin, nblk, e, pl);
+      measure_sites<Links64, false>(L, R.g, mcta - R.mcta_begin, nblk, e, pl);
   } else {
     Links32 L{B.q32 + R.link_off, R.g.vh};
     if (R.bc == BC_PMC)
-      measure_sites<Links32, true>(L, R.g, blockIdx.x - R.mcta_begin, nblk, e, pl);
+      measure_sites<Links32, true>(L, R.g, mcta - R.mcta_begin, nblk, e, pl);
     else
-      measure_sites<Links32, false>(L, R.g, blockIdx.x - R.mcta_begin, nblk, e, pl);
+      measure_sites<Links32, false>(L, R.g, mcta - R.mcta_begin, nblk, e, pl);
   }
   double se, sp;
   block_sum2(e, pl * (1.0 / 3.0), &se, &sp);
   __shared__ bool last_rep;
   if (threadIdx.x == 0) {
-    partials[blockIdx.x] = make_double2(se, sp);
+    partials[mcta] = make_double2(se, sp);
     __threadfence();
     last_rep = atomicAdd(rep_count + r, 1u) == (unsigned int)nblk - 1;
   }
@@ -205,8 +212,8 @@ __global__ void __launch_bounds__(kBlock) batch_measure(BatchView B, double2* pa
       const double scale = 1.0 / (2.0 * (double)R.g.vh);
       if (k < cap) series[(size_t)r * cap + k] = make_double2(sa * scale, sb * scale);
       rep_count[r] = 0u;
-      // the last replica to finish (every CTA of the launch done) moves the
-      // cursor: one atomic per replica, not one per CTA
+      // the last replica of the launch to finish (every CTA done) moves the
+      // cursor of the launch's replicas: one atomic per replica, not per CTA
       __threadfence();
       const bool last_all = atomicAdd(all_count, 1u) == (unsigned int)B.n - 1;
       if (last_all) {
@@ -240,6 +247,21 @@ BatchPhaseFn batch_phase_fn(int k, int kind) {
 
 }  // namespace
 
+// A group: a run of consecutive replicas swept together.  Replicas are
+// independent, so a group can go through all the sweeps of a run while its
+// links stay in L2 before the next group starts (each group with its own
+// drawing-phase counter and measurement cursor, so every replica draws and
+// records exactly what it would in one group of everything).
+// default target of link bytes per group: well inside the 126 MB L2
+constexpr long long kBatchGroupBytes = 64ll << 20;
+
+struct BatchGroup {
+  int r0, r1;         // replicas [r0, r1)
+  int cta0, ctas;     // its CTAs in the phase launches' table
+  int mcta0, mctas;   // its CTAs in the measurement's table
+  cudaGraphExec_t graph = nullptr;  // one measurement interval of this group
+};
+
 struct qcd_batch {
   std::vector<Replica> rep;
   qcd_params common;
@@ -256,19 +278,21 @@ struct qcd_batch {
   double2* hi = nullptr;
   uint32_t* rng = nullptr;
   uint32_t* mrg_jumps = nullptr;  // jump matrices that seed the streams (mrg_jump_table)
-  unsigned long long* draw_dev = nullptr;  // drawing phases run so far (FP32 draws)
+  // per group (n entries, groups use the first ones): drawing phases run so
+  // far (FP32 draws), arrival counter and cursor of the measurement
+  unsigned long long* draw_dev = nullptr;
+  unsigned int* all_count = nullptr;
+  int* cursor = nullptr;
   int* accept = nullptr;
   int* err = nullptr;
   double2* partials = nullptr;
   unsigned int* rep_count = nullptr;
-  unsigned int* all_count = nullptr;
-  int* cursor = nullptr;
   double2* series = nullptr;
   int cap = 0;
   long long sweeps_done = 0;
-  cudaGraphExec_t graph = nullptr;
+  std::vector<BatchGroup> groups;
+  long long group_bytes = 0;  // target link bytes per group (0: one group)
   int graph_every = 0;
-  int graph_renorm_phase = -1;
   char msg[512] = {0};
 };
 
@@ -294,54 +318,109 @@ int bfail(qcd_batch* b, int code, const char* fmt, ...) {
     }                                                                                               \
   } while (0)
 
+// every replica (setup, whole-batch launches)
 BatchView view(const qcd_batch* b) {
-  return BatchView{b->rep_dev, b->cta_rep, b->mcta_rep, b->n, b->q32, b->lo, b->hi, b->rng};
+  return BatchView{b->rep_dev, b->cta_rep, b->mcta_rep, b->n, 0, 0, b->q32, b->lo, b->hi, b->rng};
+}
+// the replicas of one group
+BatchView view(const qcd_batch* b, const BatchGroup& g) {
+  return BatchView{b->rep_dev, b->cta_rep, b->mcta_rep, g.r1 - g.r0, g.cta0, g.mcta0, b->q32, b->lo, b->hi, b->rng};
 }
 
 bool fp64(const qcd_batch* b) { return b->common.precision == QCD_PREC_FP64; }
 
-int batch_pass(qcd_batch* b, int kind, int renorm) {
-  BatchArgs a{b->common.epsilon, b->common.upd, b->err, b->accept, renorm, b->draw_dev, 0};
+long long link_bytes_of(const qcd_batch* b, int r) {
+  return 6ll * b->rep[r].g.vh * (fp64(b) ? 32 : 16);
+}
+
+void drop_graphs(qcd_batch* b) {
+  for (BatchGroup& g : b->groups)
+    if (g.graph) {
+      cudaGraphExecDestroy(g.graph);
+      g.graph = nullptr;
+    }
+}
+
+// consecutive replicas up to `bytes` of links per group (at least one
+// replica each); 0 puts every replica in one group
+void form_groups(qcd_batch* b, long long bytes) {
+  drop_graphs(b);
+  b->groups.clear();
+  b->group_bytes = bytes;
+  int r = 0;
+  while (r < b->n) {
+    BatchGroup g;
+    g.r0 = r;
+    long long acc = 0;
+    do {
+      acc += link_bytes_of(b, r);
+      r++;
+    } while (r < b->n && (bytes <= 0 || acc + link_bytes_of(b, r) <= bytes));
+    g.r1 = r;
+    g.cta0 = b->rep[g.r0].cta_begin;
+    g.ctas = (g.r1 < b->n ? b->rep[g.r1].cta_begin : b->ctas) - g.cta0;
+    g.mcta0 = b->rep[g.r0].mcta_begin;
+    g.mctas = (g.r1 < b->n ? b->rep[g.r1].mcta_begin : b->mctas) - g.mcta0;
+    b->groups.push_back(g);
+  }
+}
+
+// All groups hold the same counter and cursor between runs: give every
+// group slot the values of slot 0 (after the groups were formed anew).
+__global__ void spread_group_state(unsigned long long* draw, int* cursor, unsigned int* all_count, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    draw[i] = draw[0];
+    cursor[i] = cursor[0];
+    all_count[i] = 0u;
+  }
+}
+
+int batch_pass(qcd_batch* b, int gi, int kind, int renorm) {
+  const BatchGroup& g = b->groups[gi];
+  BatchArgs a{b->common.epsilon, b->common.upd, b->err, b->accept, renorm, b->draw_dev + gi, 0};
   for (int k = 0; k < 6; k++) {
     a.phase_off = (unsigned int)k;
     if (fp64(b))
-      batch_phase_fn<true>(k, kind)<<<b->ctas, kBlock, 0, b->stream>>>(view(b), a);
+      batch_phase_fn<true>(k, kind)<<<g.ctas, kBlock, 0, b->stream>>>(view(b, g), a);
     else
-      batch_phase_fn<false>(k, kind)<<<b->ctas, kBlock, 0, b->stream>>>(view(b), a);
+      batch_phase_fn<false>(k, kind)<<<g.ctas, kBlock, 0, b->stream>>>(view(b, g), a);
     BCUDA(b, cudaGetLastError());
   }
   if (kind != KIND_OR) {
-    advance_counter<<<1, 1, 0, b->stream>>>(b->draw_dev, 6ull);
+    advance_counter<<<1, 1, 0, b->stream>>>(b->draw_dev + gi, 6ull);
     BCUDA(b, cudaGetLastError());
   }
   return QCD_OK;
 }
 
-// one sweep of every replica (+ n_or over-relaxation passes; FP32 links are
-// re-projected at their last update when `renorm`, FP64 by a normalize launch)
-int batch_sweep(qcd_batch* b, bool renorm) {
+// one sweep of a group's replicas (+ n_or over-relaxation passes; FP32 links
+// are re-projected at their last update when `renorm`, FP64 by a normalize launch)
+int batch_sweep(qcd_batch* b, int gi, bool renorm) {
   const int kind = b->common.algo == QCD_ALGO_HEATBATH ? KIND_HB : KIND_METRO;
   const bool fused = renorm && !fp64(b);
-  int rc = batch_pass(b, kind, fused && b->common.n_or == 0);
-  for (int r = 0; rc == QCD_OK && r < b->common.n_or; r++) rc = batch_pass(b, KIND_OR, fused && r == b->common.n_or - 1);
+  int rc = batch_pass(b, gi, kind, fused && b->common.n_or == 0);
+  for (int r = 0; rc == QCD_OK && r < b->common.n_or; r++) rc = batch_pass(b, gi, KIND_OR, fused && r == b->common.n_or - 1);
   if (rc) return rc;
   if (renorm && !fused) {
+    const BatchGroup& g = b->groups[gi];
     if (fp64(b))
-      batch_normalize<true><<<b->ctas, kBlock, 0, b->stream>>>(view(b));
+      batch_normalize<true><<<g.ctas, kBlock, 0, b->stream>>>(view(b, g));
     else
-      batch_normalize<false><<<b->ctas, kBlock, 0, b->stream>>>(view(b));
+      batch_normalize<false><<<g.ctas, kBlock, 0, b->stream>>>(view(b, g));
     BCUDA(b, cudaGetLastError());
   }
   return QCD_OK;
 }
 
-int batch_measure_launch(qcd_batch* b) {
+int batch_measure_launch(qcd_batch* b, int gi) {
+  const BatchGroup& g = b->groups[gi];
   if (fp64(b))
-    batch_measure<true><<<b->mctas, kBlock, 0, b->stream>>>(view(b), b->partials, b->rep_count, b->all_count,
-                                                            b->cursor, b->series, b->cap);
+    batch_measure<true><<<g.mctas, kBlock, 0, b->stream>>>(view(b, g), b->partials, b->rep_count, b->all_count + gi,
+                                                           b->cursor + gi, b->series, b->cap);
   else
-    batch_measure<false><<<b->mctas, kBlock, 0, b->stream>>>(view(b), b->partials, b->rep_count, b->all_count,
-                                                             b->cursor, b->series, b->cap);
+    batch_measure<false><<<g.mctas, kBlock, 0, b->stream>>>(view(b, g), b->partials, b->rep_count,
+                                                            b->all_count + gi, b->cursor + gi, b->series, b->cap);
   BCUDA(b, cudaGetLastError());
   return QCD_OK;
 }
@@ -351,7 +430,7 @@ bool renorm_due(const qcd_batch* b, long long sweep_index) {
 }
 
 void release(qcd_batch* b) {
-  if (b->graph) cudaGraphExecDestroy(b->graph);
+  drop_graphs(b);
   cudaFree(b->rep_dev);
   cudaFree(b->cta_rep);
   cudaFree(b->mcta_rep);
@@ -471,17 +550,17 @@ int qcd_batch_create(const qcd_replica* r, int n, const qcd_params* common, qcd_
     if (rc == QCD_OK) step(cudaMemsetAsync(b->accept, 0, site_off * sizeof(int), b->stream), "memset");
   }
   if (rc == QCD_OK) step(cudaMalloc(&b->err, sizeof(int)), "cudaMalloc(err)");
-  if (rc == QCD_OK) step(cudaMalloc(&b->draw_dev, sizeof(unsigned long long)), "cudaMalloc(draw counter)");
-  if (rc == QCD_OK) step(cudaMemsetAsync(b->draw_dev, 0, sizeof(unsigned long long), b->stream), "memset");
+  if (rc == QCD_OK) step(cudaMalloc(&b->draw_dev, n * sizeof(unsigned long long)), "cudaMalloc(draw counters)");
+  if (rc == QCD_OK) step(cudaMemsetAsync(b->draw_dev, 0, n * sizeof(unsigned long long), b->stream), "memset");
   if (rc == QCD_OK)
     step(cudaMalloc(&b->partials, (size_t)(mcta > cta ? mcta : cta) * sizeof(double2)), "cudaMalloc(partials)");
   if (rc == QCD_OK) step(cudaMalloc(&b->rep_count, n * sizeof(unsigned int)), "cudaMalloc(counters)");
-  if (rc == QCD_OK) step(cudaMalloc(&b->all_count, sizeof(unsigned int)), "cudaMalloc(counters)");
-  if (rc == QCD_OK) step(cudaMalloc(&b->cursor, sizeof(int)), "cudaMalloc(cursor)");
+  if (rc == QCD_OK) step(cudaMalloc(&b->all_count, n * sizeof(unsigned int)), "cudaMalloc(counters)");
+  if (rc == QCD_OK) step(cudaMalloc(&b->cursor, n * sizeof(int)), "cudaMalloc(cursor)");
   if (rc == QCD_OK) step(cudaMemsetAsync(b->err, 0, sizeof(int), b->stream), "memset");
   if (rc == QCD_OK) step(cudaMemsetAsync(b->rep_count, 0, n * sizeof(unsigned int), b->stream), "memset");
-  if (rc == QCD_OK) step(cudaMemsetAsync(b->all_count, 0, sizeof(unsigned int), b->stream), "memset");
-  if (rc == QCD_OK) step(cudaMemsetAsync(b->cursor, 0, sizeof(int), b->stream), "memset");
+  if (rc == QCD_OK) step(cudaMemsetAsync(b->all_count, 0, n * sizeof(unsigned int), b->stream), "memset");
+  if (rc == QCD_OK) step(cudaMemsetAsync(b->cursor, 0, n * sizeof(int), b->stream), "memset");
   if (rc == QCD_OK) step(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize");
   if (rc != QCD_OK) {
     fprintf(stderr, "qcd_batch_create: %s\n", b->msg);
@@ -489,6 +568,7 @@ int qcd_batch_create(const qcd_replica* r, int n, const qcd_params* common, qcd_
     delete b;
     return rc;
   }
+  form_groups(b, kBatchGroupBytes);
   *out = b;
   return QCD_OK;
 }
@@ -505,10 +585,7 @@ int qcd_batch_set_stream(qcd_batch* b, void* stream) {
   if (!b) return QCD_ERR_INVALID;
   BCUDA(b, cudaStreamSynchronize(b->stream));
   b->stream = stream ? (cudaStream_t)stream : b->own;
-  if (b->graph) {
-    cudaGraphExecDestroy(b->graph);
-    b->graph = nullptr;
-  }
+  drop_graphs(b);
   return QCD_OK;
 }
 
@@ -519,10 +596,10 @@ int qcd_batch_init(qcd_batch* b) {
   else
     batch_setup<false><<<b->ctas, kBlock, 0, b->stream>>>(view(b), b->mrg_jumps);
   BCUDA(b, cudaGetLastError());
-  BCUDA(b, cudaMemsetAsync(b->cursor, 0, sizeof(int), b->stream));
+  BCUDA(b, cudaMemsetAsync(b->cursor, 0, b->n * sizeof(int), b->stream));
   // a fresh start: the streams are re-seeded above, the counter of the FP32
   // draws starts again at 0 (as for a newly created lattice)
-  BCUDA(b, cudaMemsetAsync(b->draw_dev, 0, sizeof(unsigned long long), b->stream));
+  BCUDA(b, cudaMemsetAsync(b->draw_dev, 0, b->n * sizeof(unsigned long long), b->stream));
   b->sweeps_done = 0;
   return QCD_OK;
 }
@@ -533,15 +610,12 @@ int qcd_batch_reserve(qcd_batch* b, int capacity) {
   cudaFree(b->series);
   b->series = nullptr;
   b->cap = 0;
-  if (b->graph) {  // the graph holds the old series pointer
-    cudaGraphExecDestroy(b->graph);
-    b->graph = nullptr;
-  }
+  drop_graphs(b);  // the graphs hold the old series pointer
   if (capacity) {
     BCUDA(b, cudaMalloc(&b->series, (size_t)capacity * b->n * sizeof(double2)));
     BCUDA(b, cudaMemsetAsync(b->series, 0, (size_t)capacity * b->n * sizeof(double2), b->stream));
   }
-  BCUDA(b, cudaMemsetAsync(b->cursor, 0, sizeof(int), b->stream));
+  BCUDA(b, cudaMemsetAsync(b->cursor, 0, b->n * sizeof(int), b->stream));
   b->cap = capacity;
   return QCD_OK;
 }
@@ -550,47 +624,172 @@ int qcd_batch_run(qcd_batch* b, int sweeps, int measure_every, int use_graph) {
   if (!b || sweeps < 0 || measure_every < 0) return QCD_ERR_INVALID;
   if (measure_every > 0 && b->cap == 0) return bfail(b, QCD_ERR_INVALID, "reserve a series before measuring");
   int rc = QCD_OK;
-  // a graph of one measurement interval; its re-projection pattern must not
-  // vary between replays, so it is used when renorm_every divides the interval
+  // a graph of one measurement interval per group; its re-projection pattern
+  // must not vary between replays, so it is used when renorm_every divides
+  // the interval
   const int every = measure_every > 0 ? measure_every : 1;
   const bool graphable = use_graph && measure_every > 0 &&
                          (b->common.renorm_every == 0 || every % b->common.renorm_every == 0) &&
                          b->sweeps_done % every == 0 &&
                          (b->common.renorm_every == 0 || b->sweeps_done % b->common.renorm_every == 0);
-  int done = 0;
-  if (graphable && sweeps >= every) {
-    if (!b->graph || b->graph_every != every) {
-      if (b->graph) cudaGraphExecDestroy(b->graph);
-      b->graph = nullptr;
-      cudaGraph_t g;
-      BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-      for (int s = 0; rc == QCD_OK && s < every; s++) rc = batch_sweep(b, renorm_due(b, s));
-      if (rc == QCD_OK) rc = batch_measure_launch(b);
-      cudaError_t e = cudaStreamEndCapture(b->stream, &g);
-      if (rc) {
-        if (e == cudaSuccess) cudaGraphDestroy(g);
-        return rc;
+  if (graphable && b->graph_every != every) {
+    drop_graphs(b);
+    b->graph_every = every;
+  }
+  // every group goes through all the sweeps before the next one starts
+  for (int gi = 0; gi < (int)b->groups.size(); gi++) {
+    BatchGroup& G = b->groups[gi];
+    long long swept = b->sweeps_done;
+    int done = 0;
+    if (graphable && sweeps >= every) {
+      if (!G.graph) {
+        cudaGraph_t g;
+        BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        for (int s = 0; rc == QCD_OK && s < every; s++) rc = batch_sweep(b, gi, renorm_due(b, s));
+        if (rc == QCD_OK) rc = batch_measure_launch(b, gi);
+        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        if (rc) {
+          if (e == cudaSuccess) cudaGraphDestroy(g);
+          return rc;
+        }
+        BCUDA(b, e);
+        e = cudaGraphInstantiate(&G.graph, g, 0);
+        cudaGraphDestroy(g);
+        BCUDA(b, e);
       }
-      BCUDA(b, e);
-      e = cudaGraphInstantiate(&b->graph, g, 0);
-      cudaGraphDestroy(g);
-      BCUDA(b, e);
-      b->graph_every = every;
+      for (; done + every <= sweeps; done += every) {
+        BCUDA(b, cudaGraphLaunch(G.graph, b->stream));
+        swept += every;
+      }
     }
-    for (; done + every <= sweeps; done += every) {
-      BCUDA(b, cudaGraphLaunch(b->graph, b->stream));
-      b->sweeps_done += every;
-    }
-  }
-  for (; done < sweeps; done++) {
-    rc = batch_sweep(b, renorm_due(b, b->sweeps_done));
-    if (rc) return rc;
-    b->sweeps_done++;
-    if (measure_every > 0 && b->sweeps_done % measure_every == 0) {
-      rc = batch_measure_launch(b);
+    for (; done < sweeps; done++) {
+      rc = batch_sweep(b, gi, renorm_due(b, swept));
       if (rc) return rc;
+      swept++;
+      if (measure_every > 0 && swept % measure_every == 0) {
+        rc = batch_measure_launch(b, gi);
+        if (rc) return rc;
+      }
     }
   }
+  b->sweeps_done += sweeps;
+  return QCD_OK;
+}
+
+int qcd_batch_set_groups(qcd_batch* b, long long bytes_per_group) {
+  if (!b || bytes_per_group < 0) return QCD_ERR_INVALID;
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  form_groups(b, bytes_per_group);
+  // the new groups start from the common counter and cursor of the old ones
+  spread_group_state<<<(b->n + 255) / 256, 256, 0, b->stream>>>(b->draw_dev, b->cursor, b->all_count, b->n);
+  BCUDA(b, cudaGetLastError());
+  return QCD_OK;
+}
+
+int qcd_batch_groups(const qcd_batch* b) { return b ? (int)b->groups.size() : QCD_ERR_INVALID; }
+
+int qcd_batch_autotune(qcd_batch* b, int sweeps_per_trial, long long* bytes_out, double* ms_out) {
+  if (!b || sweeps_per_trial < 0) return QCD_ERR_INVALID;
+  if (sweeps_per_trial == 0) sweeps_per_trial = 20;
+  BCUDA(b, cudaStreamSynchronize(b->stream));
+  // the trials advance the batch: save links, streams, counters, cursors and
+  // series, restore them afterwards
+  struct Saved {
+    void *l0 = nullptr, *l1 = nullptr, *rng = nullptr, *acc = nullptr, *draw = nullptr, *cur = nullptr,
+         *ser = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ~Saved() {
+      cudaFree(l0);
+      cudaFree(l1);
+      cudaFree(rng);
+      cudaFree(acc);
+      cudaFree(draw);
+      cudaFree(cur);
+      cudaFree(ser);
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+    }
+  } sv;
+  long long links = 0;
+  for (int r = 0; r < b->n; r++) links += link_bytes_of(b, r);
+  const size_t lb = fp64(b) ? (size_t)links / 2 : (size_t)links;  // per store (FP64: lo and hi)
+  const size_t rngb = (size_t)(b->sites / 2) * 6 * sizeof(uint32_t);
+  const size_t serb = (size_t)b->cap * b->n * sizeof(double2);
+  void* L0 = fp64(b) ? (void*)b->lo : (void*)b->q32;
+  BCUDA(b, cudaMalloc(&sv.l0, lb));
+  BCUDA(b, cudaMemcpyAsync(sv.l0, L0, lb, cudaMemcpyDeviceToDevice, b->stream));
+  if (fp64(b)) {
+    BCUDA(b, cudaMalloc(&sv.l1, lb));
+    BCUDA(b, cudaMemcpyAsync(sv.l1, b->hi, lb, cudaMemcpyDeviceToDevice, b->stream));
+    BCUDA(b, cudaMalloc(&sv.rng, rngb));
+    BCUDA(b, cudaMemcpyAsync(sv.rng, b->rng, rngb, cudaMemcpyDeviceToDevice, b->stream));
+  }
+  if (b->accept) {
+    BCUDA(b, cudaMalloc(&sv.acc, (size_t)b->sites * sizeof(int)));
+    BCUDA(b, cudaMemcpyAsync(sv.acc, b->accept, (size_t)b->sites * sizeof(int), cudaMemcpyDeviceToDevice, b->stream));
+  }
+  BCUDA(b, cudaMalloc(&sv.draw, b->n * sizeof(unsigned long long)));
+  BCUDA(b, cudaMemcpyAsync(sv.draw, b->draw_dev, b->n * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, b->stream));
+  BCUDA(b, cudaMalloc(&sv.cur, b->n * sizeof(int)));
+  BCUDA(b, cudaMemcpyAsync(sv.cur, b->cursor, b->n * sizeof(int), cudaMemcpyDeviceToDevice, b->stream));
+  if (serb) {
+    BCUDA(b, cudaMalloc(&sv.ser, serb));
+    BCUDA(b, cudaMemcpyAsync(sv.ser, b->series, serb, cudaMemcpyDeviceToDevice, b->stream));
+  }
+  BCUDA(b, cudaEventCreate(&sv.e0));
+  BCUDA(b, cudaEventCreate(&sv.e1));
+  const long long swept = b->sweeps_done, bytes_save = b->group_bytes;
+  // candidates: one group of everything and groups of 128 .. 16 MB of links
+  const long long cand[] = {0, 128ll << 20, 96ll << 20, 64ll << 20, 48ll << 20, 32ll << 20, 16ll << 20};
+  const int measure = b->cap > 0 ? 1 : 0;
+  long long best = bytes_save;
+  double best_ms = 1e300;
+  int rc = QCD_OK, last_groups = -1;
+  for (long long c : cand) {
+    rc = qcd_batch_set_groups(b, c);
+    if (rc) break;
+    if ((int)b->groups.size() == last_groups) continue;  // the same partition as the previous candidate
+    last_groups = (int)b->groups.size();
+    rc = qcd_batch_run(b, 1, measure, measure);  // builds the graphs
+    if (rc) break;
+    if (cudaEventRecord(sv.e0, b->stream) != cudaSuccess) {
+      rc = bfail(b, QCD_ERR_CUDA, "autotune: event record");
+      break;
+    }
+    rc = qcd_batch_run(b, sweeps_per_trial, measure, measure);
+    if (rc) break;
+    if (cudaEventRecord(sv.e1, b->stream) != cudaSuccess || cudaEventSynchronize(sv.e1) != cudaSuccess) {
+      rc = bfail(b, QCD_ERR_CUDA, "autotune: event wait");
+      break;
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, sv.e0, sv.e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  // restore the batch as it was
+  cudaMemcpyAsync(L0, sv.l0, lb, cudaMemcpyDeviceToDevice, b->stream);
+  if (fp64(b)) {
+    cudaMemcpyAsync(b->hi, sv.l1, lb, cudaMemcpyDeviceToDevice, b->stream);
+    cudaMemcpyAsync(b->rng, sv.rng, rngb, cudaMemcpyDeviceToDevice, b->stream);
+  }
+  if (sv.acc) cudaMemcpyAsync(b->accept, sv.acc, (size_t)b->sites * sizeof(int), cudaMemcpyDeviceToDevice, b->stream);
+  cudaMemcpyAsync(b->draw_dev, sv.draw, b->n * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, b->stream);
+  cudaMemcpyAsync(b->cursor, sv.cur, b->n * sizeof(int), cudaMemcpyDeviceToDevice, b->stream);
+  cudaMemsetAsync(b->all_count, 0, b->n * sizeof(unsigned int), b->stream);
+  if (serb) cudaMemcpyAsync(b->series, sv.ser, serb, cudaMemcpyDeviceToDevice, b->stream);
+  cudaStreamSynchronize(b->stream);
+  b->sweeps_done = swept;
+  if (rc) {
+    form_groups(b, bytes_save);
+    return rc;
+  }
+  form_groups(b, best);
+  if (bytes_out) *bytes_out = best;
+  if (ms_out) *ms_out = best_ms / sweeps_per_trial;
+  BCUDA(b, cudaGetLastError());
   return QCD_OK;
 }
 

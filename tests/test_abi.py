@@ -102,3 +102,10 @@ def test_noalloc_measurement_refuses_on_the_host():
     assert lib.qcd_measure_aos_noalloc(fake, 8, 6, 5, 0, fake, None) == -1
     assert lib.qcd_measure_aos_noalloc(fake, 8, 8, 8, -1, fake, None) == -1
     assert lib.qcd_measure_aos_noalloc(fake, 8, 8, 8, 0, None, None) == -1
+
+
+def test_batch_refuses_stream_offsets_beyond_the_seeding_tables():
+    # the streams of a replica are seeded by jumps of up to 2^40 subsequences
+    with pytest.raises(q.QcdError) as ei:
+        q.Batch([dict(lt=4, lx=4, ly=4, beta=5.0, stream_offset=(1 << 40) - 10)])
+    assert ei.value.status == -1

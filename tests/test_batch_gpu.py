@@ -78,3 +78,50 @@ def test_batch_of_96_uneven_replicas_runs_and_thermalises():
         e, p = B.series(i)
         assert np.all(np.isfinite(p)) and 0.2 < p[-1] < 1.0
     B.close()
+
+
+@pytest.mark.parametrize("precision,algo,n_or", [("fp32", "hb", 1), ("fp64", "metro", 0)])
+def test_groups_give_the_same_results_as_one_group(precision, algo, n_or):
+    # one replica per group (1 byte per group), then a regrouping in the middle
+    # of the run: every replica draws and records exactly as in one group
+    kw = dict(algo=algo, precision=precision, epsilon=0.25, upd=2, n_or=n_or,
+              renorm_every=1 if precision == "fp32" else 0)
+    A, G = q.Batch(REPS, **kw), q.Batch(REPS, **kw)
+    A.set_groups(0)
+    G.set_groups(1)
+    assert A.groups() == 1 and G.groups() == len(REPS)
+    for B in (A, G):
+        B.init()
+        B.reserve(10)
+        B.run(4, measure_every=1, graph=True)
+    G.set_groups(3 * 1024 * 16)
+    for B in (A, G):
+        B.run(4, measure_every=2, graph=False)
+        B.run(2, measure_every=1, graph=True)
+    assert A.measured() == G.measured() == 8
+    for i in range(len(REPS)):
+        ea, pa = A.series(i, 8)
+        eg, pg = G.series(i, 8)
+        assert np.array_equal(ea, eg) and np.array_equal(pa, pg)
+        assert np.array_equal(A.store_config(i), G.store_config(i))
+    A.close()
+    G.close()
+
+
+def test_batch_autotune_restores_the_batch():
+    kw = dict(algo="hb", precision="fp32", renorm_every=1)
+    A, T = q.Batch(REPS, **kw), q.Batch(REPS, **kw)
+    for B in (A, T):
+        B.init()
+        B.reserve(12)
+        B.run(3, measure_every=1)
+    t = T.autotune(4)
+    assert t["groups"] >= 1 and t["ms_per_sweep"] > 0
+    assert T.measured() == 3
+    for B in (A, T):
+        B.run(3, measure_every=1)
+    for i in range(len(REPS)):
+        assert np.array_equal(A.series(i, 6)[1], T.series(i, 6)[1])
+        assert np.array_equal(A.store_config(i), T.store_config(i))
+    A.close()
+    T.close()
