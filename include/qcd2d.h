@@ -286,12 +286,19 @@ int qcd_batch_run(qcd_batch* b, int sweeps, int measure_every, int use_graph);
 int qcd_batch_set_groups(qcd_batch* b, long long bytes_per_group);
 /* number of groups */
 int qcd_batch_groups(const qcd_batch* b);
+/* Lanes (1..4, default 1): streams on which groups run at the same time,
+   group g on lane g mod lanes, forked from and joined back into the batch's
+   stream; one group's memory-bound measurement then overlaps another's
+   phases. */
+int qcd_batch_set_lanes(qcd_batch* b, int lanes);
 /* Autotuner of the grouping: times sweeps_per_trial sweeps (0: 20; with a
    measurement after each when a series is reserved, as CUDA graphs) for one
-   group of everything and groups of 128 to 16 MB of links, restores the
-   batch's links, streams, counters, cursors and series exactly, and keeps the
-   fastest grouping (its bytes and ms per sweep, when the pointers are not NULL). */
-int qcd_batch_autotune(qcd_batch* b, int sweeps_per_trial, long long* bytes_out, double* ms_per_sweep_out);
+   group of everything, the batch cut in 2-4 equal groups on as many lanes,
+   and groups of 128-32 MB of links on 1, 2 or 4 lanes; restores the batch's
+   links, streams, counters, cursors and series exactly, and keeps the fastest
+   (its bytes per group, lanes and ms per sweep, where the pointers are not NULL). */
+int qcd_batch_autotune(qcd_batch* b, int sweeps_per_trial, long long* bytes_out, int* lanes_out,
+                       double* ms_per_sweep_out);
 /* wait for the batch's stream; reports device-side errors */
 int qcd_batch_synchronize(qcd_batch* b);
 /* measurements taken so far (per replica) */

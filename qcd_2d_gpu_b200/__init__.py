@@ -172,7 +172,8 @@ _SIGS = {
     "qcd_batch_synchronize": (_I, [_P]),
     "qcd_batch_set_groups": (_I, [_P, ctypes.c_longlong]),
     "qcd_batch_groups": (_I, [_P]),
-    "qcd_batch_autotune": (_I, [_P, _I, ctypes.POINTER(ctypes.c_longlong), _DP]),
+    "qcd_batch_set_lanes": (_I, [_P, _I]),
+    "qcd_batch_autotune": (_I, [_P, _I, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int), _DP]),
     "qcd_batch_measured": (_I, [_P]),
     "qcd_batch_series": (_I, [_P, _I, _P, _P, _I]),
     "qcd_batch_store_config": (_I, [_P, _I, _P]),
@@ -455,12 +456,16 @@ class Batch:
     def groups(self):
         return self._lib.qcd_batch_groups(self._h)
 
+    def set_lanes(self, lanes):
+        """Run groups on this many streams at the same time (1..4)."""
+        self._check(self._lib.qcd_batch_set_lanes(self._h, int(lanes)), "set_lanes")
+
     def autotune(self, sweeps_per_trial=0):
-        """Pick the fastest grouping (the batch's state is preserved)."""
-        nb, ms = ctypes.c_longlong(), ctypes.c_double()
-        self._check(self._lib.qcd_batch_autotune(self._h, sweeps_per_trial, ctypes.byref(nb), ctypes.byref(ms)),
-                    "autotune")
-        return {"bytes_per_group": nb.value, "groups": self.groups(), "ms_per_sweep": ms.value}
+        """Pick the fastest grouping and lanes (the batch's state is preserved)."""
+        nb, nl, ms = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_double()
+        self._check(self._lib.qcd_batch_autotune(self._h, sweeps_per_trial, ctypes.byref(nb), ctypes.byref(nl),
+                                                 ctypes.byref(ms)), "autotune")
+        return {"bytes_per_group": nb.value, "groups": self.groups(), "lanes": nl.value, "ms_per_sweep": ms.value}
 
     def measured(self):
         k = self._lib.qcd_batch_measured(self._h)

@@ -19,6 +19,7 @@
 #include <string.h>
 
 #include <new>
+#include <utility>
 #include <vector>
 
 #include "qcd2d.h"
@@ -292,6 +293,12 @@ struct qcd_batch {
   long long sweeps_done = 0;
   std::vector<BatchGroup> groups;
   long long group_bytes = 0;  // target link bytes per group (0: one group)
+  // lanes: streams that run groups concurrently (group g on lane g mod lanes),
+  // forked from and joined back into `stream` by events
+  static constexpr int kMaxLanes = 4;
+  int lanes = 1;
+  cudaStream_t lane[kMaxLanes] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t fork_ev = nullptr, join_ev[kMaxLanes] = {nullptr, nullptr, nullptr, nullptr};
   int graph_every = 0;
   char msg[512] = {0};
 };
@@ -447,6 +454,11 @@ void release(qcd_batch* b) {
   cudaFree(b->all_count);
   cudaFree(b->cursor);
   cudaFree(b->series);
+  for (int k = 0; k < qcd_batch::kMaxLanes; k++) {
+    if (b->lane[k]) cudaStreamDestroy(b->lane[k]);
+    if (b->join_ev[k]) cudaEventDestroy(b->join_ev[k]);
+  }
+  if (b->fork_ev) cudaEventDestroy(b->fork_ev);
   if (b->own) cudaStreamDestroy(b->own);
 }
 
@@ -512,6 +524,11 @@ int qcd_batch_create(const qcd_replica* r, int n, const qcd_params* common, qcd_
   };
   step(cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking), "cudaStreamCreate");
   b->stream = b->own;
+  for (int k = 0; k < qcd_batch::kMaxLanes; k++) {
+    if (rc == QCD_OK) step(cudaStreamCreateWithFlags(&b->lane[k], cudaStreamNonBlocking), "cudaStreamCreate(lane)");
+    if (rc == QCD_OK) step(cudaEventCreateWithFlags(&b->join_ev[k], cudaEventDisableTiming), "cudaEventCreate");
+  }
+  if (rc == QCD_OK) step(cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming), "cudaEventCreate");
   if (rc == QCD_OK) step(cudaMalloc(&b->rep_dev, n * sizeof(Replica)), "cudaMalloc(replicas)");
   if (rc == QCD_OK)
     step(cudaMemcpy(b->rep_dev, b->rep.data(), n * sizeof(Replica), cudaMemcpyHostToDevice), "replica table");
@@ -636,43 +653,70 @@ int qcd_batch_run(qcd_batch* b, int sweeps, int measure_every, int use_graph) {
     drop_graphs(b);
     b->graph_every = every;
   }
-  // every group goes through all the sweeps before the next one starts
-  for (int gi = 0; gi < (int)b->groups.size(); gi++) {
+  // every group goes through all the sweeps before the next one starts on
+  // its lane; with several lanes the groups of different lanes run at the
+  // same time (one group's measurement next to another group's phases)
+  const int lanes = b->lanes < (int)b->groups.size() ? b->lanes : (int)b->groups.size();
+  cudaStream_t main = b->stream;
+  if (lanes > 1) {
+    BCUDA(b, cudaEventRecord(b->fork_ev, main));
+    for (int k = 0; k < lanes; k++) BCUDA(b, cudaStreamWaitEvent(b->lane[k], b->fork_ev, 0));
+  }
+  for (int gi = 0; gi < (int)b->groups.size() && rc == QCD_OK; gi++) {
     BatchGroup& G = b->groups[gi];
+    b->stream = lanes > 1 ? b->lane[gi % lanes] : main;  // the launch helpers use b->stream
     long long swept = b->sweeps_done;
     int done = 0;
     if (graphable && sweeps >= every) {
       if (!G.graph) {
         cudaGraph_t g;
-        BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) {
+          rc = bfail(b, QCD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+          break;
+        }
         for (int s = 0; rc == QCD_OK && s < every; s++) rc = batch_sweep(b, gi, renorm_due(b, s));
         if (rc == QCD_OK) rc = batch_measure_launch(b, gi);
-        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        e = cudaStreamEndCapture(b->stream, &g);
         if (rc) {
           if (e == cudaSuccess) cudaGraphDestroy(g);
-          return rc;
+          break;
         }
-        BCUDA(b, e);
-        e = cudaGraphInstantiate(&G.graph, g, 0);
-        cudaGraphDestroy(g);
-        BCUDA(b, e);
+        if (e == cudaSuccess) {
+          e = cudaGraphInstantiate(&G.graph, g, 0);
+          cudaGraphDestroy(g);
+        }
+        if (e != cudaSuccess) {
+          rc = bfail(b, QCD_ERR_CUDA, "graph: %s", cudaGetErrorString(e));
+          break;
+        }
       }
-      for (; done + every <= sweeps; done += every) {
-        BCUDA(b, cudaGraphLaunch(G.graph, b->stream));
+      for (; done + every <= sweeps && rc == QCD_OK; done += every) {
+        if (cudaGraphLaunch(G.graph, b->stream) != cudaSuccess) rc = bfail(b, QCD_ERR_CUDA, "graph launch");
         swept += every;
       }
     }
-    for (; done < sweeps; done++) {
+    for (; done < sweeps && rc == QCD_OK; done++) {
       rc = batch_sweep(b, gi, renorm_due(b, swept));
-      if (rc) return rc;
       swept++;
-      if (measure_every > 0 && swept % measure_every == 0) {
-        rc = batch_measure_launch(b, gi);
-        if (rc) return rc;
-      }
+      if (rc == QCD_OK && measure_every > 0 && swept % measure_every == 0) rc = batch_measure_launch(b, gi);
     }
   }
+  b->stream = main;
+  if (lanes > 1) {
+    for (int k = 0; k < lanes; k++) {
+      cudaEventRecord(b->join_ev[k], b->lane[k]);
+      cudaStreamWaitEvent(main, b->join_ev[k], 0);
+    }
+  }
+  if (rc) return rc;
   b->sweeps_done += sweeps;
+  return QCD_OK;
+}
+
+int qcd_batch_set_lanes(qcd_batch* b, int lanes) {
+  if (!b || lanes < 1 || lanes > qcd_batch::kMaxLanes) return QCD_ERR_INVALID;
+  b->lanes = lanes;
   return QCD_OK;
 }
 
@@ -688,7 +732,7 @@ int qcd_batch_set_groups(qcd_batch* b, long long bytes_per_group) {
 
 int qcd_batch_groups(const qcd_batch* b) { return b ? (int)b->groups.size() : QCD_ERR_INVALID; }
 
-int qcd_batch_autotune(qcd_batch* b, int sweeps_per_trial, long long* bytes_out, double* ms_out) {
+int qcd_batch_autotune(qcd_batch* b, int sweeps_per_trial, long long* bytes_out, int* lanes_out, double* ms_out) {
   if (!b || sweeps_per_trial < 0) return QCD_ERR_INVALID;
   if (sweeps_per_trial == 0) sweeps_per_trial = 20;
   BCUDA(b, cudaStreamSynchronize(b->stream));
@@ -739,17 +783,33 @@ int qcd_batch_autotune(qcd_batch* b, int sweeps_per_trial, long long* bytes_out,
   BCUDA(b, cudaEventCreate(&sv.e0));
   BCUDA(b, cudaEventCreate(&sv.e1));
   const long long swept = b->sweeps_done, bytes_save = b->group_bytes;
-  // candidates: one group of everything and groups of 128 .. 16 MB of links
-  const long long cand[] = {0, 128ll << 20, 96ll << 20, 64ll << 20, 48ll << 20, 32ll << 20, 16ll << 20};
+  const int lanes_save = b->lanes;
+  // candidates (bytes per group, lanes): one group of everything; the batch
+  // cut in 2-4 equal groups run side by side; L2-sized groups one after the
+  // other or two at a time
+  struct Cand {
+    long long bytes;
+    int lanes;
+  };
+  const long long T = links;
+  const Cand cand[] = {{0, 1},           {T / 2 + 1, 2},     {T / 3 + 1, 3},     {T / 4 + 1, 4},
+                       {128ll << 20, 1}, {64ll << 20, 1},    {32ll << 20, 1},    {128ll << 20, 2},
+                       {64ll << 20, 2},  {32ll << 20, 2},    {64ll << 20, 4}};
   const int measure = b->cap > 0 ? 1 : 0;
   long long best = bytes_save;
+  int best_lanes = lanes_save;
   double best_ms = 1e300;
-  int rc = QCD_OK, last_groups = -1;
-  for (long long c : cand) {
-    rc = qcd_batch_set_groups(b, c);
+  int rc = QCD_OK;
+  std::vector<std::pair<int, int>> seen;  // (groups, lanes) already timed
+  for (const Cand& c : cand) {
+    rc = qcd_batch_set_groups(b, c.bytes);
     if (rc) break;
-    if ((int)b->groups.size() == last_groups) continue;  // the same partition as the previous candidate
-    last_groups = (int)b->groups.size();
+    const int ng = (int)b->groups.size(), nl = c.lanes < ng ? c.lanes : ng;
+    bool dup = false;
+    for (auto& p : seen) dup |= p.first == ng && p.second == nl;
+    if (dup) continue;
+    seen.push_back({ng, nl});
+    b->lanes = nl;
     rc = qcd_batch_run(b, 1, measure, measure);  // builds the graphs
     if (rc) break;
     if (cudaEventRecord(sv.e0, b->stream) != cudaSuccess) {
@@ -766,7 +826,8 @@ int qcd_batch_autotune(qcd_batch* b, int sweeps_per_trial, long long* bytes_out,
     cudaEventElapsedTime(&ms, sv.e0, sv.e1);
     if (ms < best_ms) {
       best_ms = ms;
-      best = c;
+      best = c.bytes;
+      best_lanes = nl;
     }
   }
   // restore the batch as it was
@@ -784,10 +845,13 @@ int qcd_batch_autotune(qcd_batch* b, int sweeps_per_trial, long long* bytes_out,
   b->sweeps_done = swept;
   if (rc) {
     form_groups(b, bytes_save);
+    b->lanes = lanes_save;
     return rc;
   }
   form_groups(b, best);
+  b->lanes = best_lanes;
   if (bytes_out) *bytes_out = best;
+  if (lanes_out) *lanes_out = best_lanes;
   if (ms_out) *ms_out = best_ms / sweeps_per_trial;
   BCUDA(b, cudaGetLastError());
   return QCD_OK;

@@ -82,13 +82,15 @@ def test_batch_of_96_uneven_replicas_runs_and_thermalises():
 
 @pytest.mark.parametrize("precision,algo,n_or", [("fp32", "hb", 1), ("fp64", "metro", 0)])
 def test_groups_give_the_same_results_as_one_group(precision, algo, n_or):
-    # one replica per group (1 byte per group), then a regrouping in the middle
-    # of the run: every replica draws and records exactly as in one group
+    # one replica per group (1 byte per group) on three lanes, then a
+    # regrouping in the middle of the run: every replica draws and records
+    # exactly as in one group
     kw = dict(algo=algo, precision=precision, epsilon=0.25, upd=2, n_or=n_or,
               renorm_every=1 if precision == "fp32" else 0)
     A, G = q.Batch(REPS, **kw), q.Batch(REPS, **kw)
     A.set_groups(0)
     G.set_groups(1)
+    G.set_lanes(3)  # groups on three streams at once
     assert A.groups() == 1 and G.groups() == len(REPS)
     for B in (A, G):
         B.init()
