@@ -278,7 +278,7 @@ int qcd_batch_reserve(qcd_batch* b, int capacity);
 int qcd_batch_run(qcd_batch* b, int sweeps, int measure_every, int use_graph);
 /* Groups: the replicas are swept in groups of consecutive replicas holding
    at most bytes_per_group bytes of links (at least one replica each; 0: one
-   group of everything; default 64 MB), each group going through all the
+   group of everything; default 32 MB), each group going through all the
    sweeps of a qcd_batch_run while its links stay in L2 before the next group
    starts.  Replicas are independent and every group keeps its own
    drawing-phase counter and measurement cursor, so the results do not depend
@@ -286,15 +286,15 @@ int qcd_batch_run(qcd_batch* b, int sweeps, int measure_every, int use_graph);
 int qcd_batch_set_groups(qcd_batch* b, long long bytes_per_group);
 /* number of groups */
 int qcd_batch_groups(const qcd_batch* b);
-/* Lanes (1..4, default 1): streams on which groups run at the same time,
+/* Lanes (1..4, default 2): streams on which groups run at the same time,
    group g on lane g mod lanes, forked from and joined back into the batch's
    stream; one group's memory-bound measurement then overlaps another's
    phases. */
 int qcd_batch_set_lanes(qcd_batch* b, int lanes);
 /* Autotuner of the grouping: times sweeps_per_trial sweeps (0: 20; with a
    measurement after each when a series is reserved, as CUDA graphs) for one
-   group of everything, the batch cut in 2-4 equal groups on as many lanes,
-   and groups of 128-32 MB of links on 1, 2 or 4 lanes; restores the batch's
+   group of everything, the batch cut in halves on two lanes, and groups of
+   128-16 MB of links on 1 to 4 lanes; restores the batch's
    links, streams, counters, cursors and series exactly, and keeps the fastest
    (its bytes per group, lanes and ms per sweep, where the pointers are not NULL). */
 int qcd_batch_autotune(qcd_batch* b, int sweeps_per_trial, long long* bytes_out, int* lanes_out,

@@ -253,8 +253,10 @@ BatchPhaseFn batch_phase_fn(int k, int kind) {
 // links stay in L2 before the next group starts (each group with its own
 // drawing-phase counter and measurement cursor, so every replica draws and
 // records exactly what it would in one group of everything).
-// default target of link bytes per group: well inside the 126 MB L2
-constexpr long long kBatchGroupBytes = 64ll << 20;
+// default grouping (the autotuner's choice for 96 mixed replicas, C4): groups
+// of up to 32 MB of links, well inside the 126 MB L2, two at a time
+constexpr long long kBatchGroupBytes = 32ll << 20;
+constexpr int kBatchLanes = 2;
 
 struct BatchGroup {
   int r0, r1;         // replicas [r0, r1)
@@ -296,7 +298,7 @@ struct qcd_batch {
   // lanes: streams that run groups concurrently (group g on lane g mod lanes),
   // forked from and joined back into `stream` by events
   static constexpr int kMaxLanes = 4;
-  int lanes = 1;
+  int lanes = kBatchLanes;
   cudaStream_t lane[kMaxLanes] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t fork_ev = nullptr, join_ev[kMaxLanes] = {nullptr, nullptr, nullptr, nullptr};
   int graph_every = 0;
@@ -785,16 +787,16 @@ int qcd_batch_autotune(qcd_batch* b, int sweeps_per_trial, long long* bytes_out,
   const long long swept = b->sweeps_done, bytes_save = b->group_bytes;
   const int lanes_save = b->lanes;
   // candidates (bytes per group, lanes): one group of everything; the batch
-  // cut in 2-4 equal groups run side by side; L2-sized groups one after the
-  // other or two at a time
+  // cut in two halves side by side; L2-sized groups one after the other or
+  // two to four at a time
   struct Cand {
     long long bytes;
     int lanes;
   };
   const long long T = links;
-  const Cand cand[] = {{0, 1},           {T / 2 + 1, 2},     {T / 3 + 1, 3},     {T / 4 + 1, 4},
-                       {128ll << 20, 1}, {64ll << 20, 1},    {32ll << 20, 1},    {128ll << 20, 2},
-                       {64ll << 20, 2},  {32ll << 20, 2},    {64ll << 20, 4}};
+  const Cand cand[] = {{0, 1},          {T / 2 + 1, 2},  {128ll << 20, 1}, {64ll << 20, 1},  {32ll << 20, 1},
+                       {64ll << 20, 2}, {48ll << 20, 2}, {32ll << 20, 2},  {24ll << 20, 2},  {16ll << 20, 2},
+                       {32ll << 20, 3}, {32ll << 20, 4}, {16ll << 20, 3},  {16ll << 20, 4}};
   const int measure = b->cap > 0 ? 1 : 0;
   long long best = bytes_save;
   int best_lanes = lanes_save;
