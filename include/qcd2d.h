@@ -173,6 +173,21 @@ enum qcd_schedule { QCD_SCHED_AUTO = 0, QCD_SCHED_PHASES = 1, QCD_SCHED_WAVEFRON
 int qcd_set_schedule(qcd_lattice* h, int mode);
 /* the schedule qcd_sweep will use (PHASES, WAVEFRONT or PAIRS) */
 int qcd_get_schedule(const qcd_lattice* h);
+/* FP32 store layout.  An FP32 lattice with Lt % 4 == 0 keeps its links in
+   site pairs under the per-phase schedule: site id (t < Lt/2) and site
+   id + V/4 (t + Lt/2) of a link class share one 32-B record (w0 w1 x0 x1)
+   (y0 y1 z0 z1), and one thread updates both with packed two-lane FP32
+   arithmetic (about half the instructions per link update).  Same updates
+   and draws as one float4 plane per class; results agree with it to float
+   rounding.  on = 0 keeps such a lattice on one float4 plane per class (the
+   layout of the wavefront and fused-pair schedules and of the batched
+   replicas, and the one those are bit-identical to); on = 1 (the default)
+   allows the pairs.  The store is rewritten at once if the layout changes
+   (values kept exactly).  Not a reference interface: the reference stores
+   FP64 AoS only (kernel.cu:58, 78). */
+int qcd_set_pair_layout(qcd_lattice* h, int on);
+/* 1 if the FP32 store is in site pairs now, 0 if not (FP64: 0) */
+int qcd_get_pair_layout(const qcd_lattice* h);
 /* Fused pairs: streamed slices per CTA (0: automatic, enough CTAs for every
    SM several times over). */
 int qcd_set_pair_tuning(qcd_lattice* h, int slices_per_cta);
@@ -233,7 +248,8 @@ long long qcd_volume(const qcd_lattice* h);
 int qcd_get_params(const qcd_lattice* h, qcd_params* out);
 /* Device pointer and byte size of the current link store (diagnostics,
    benchmarks).  Under QCD_SCHED_PAIRS each pass moves the links to the other
-   of two stores, so the pointer holds until the next sweep. */
+   of two stores, so the pointer holds until the next sweep.  An FP32 store
+   is in site pairs when qcd_get_pair_layout says so. */
 int qcd_link_store(const qcd_lattice* h, void** dev_ptr, size_t* bytes);
 
 const char* qcd_last_error(const qcd_lattice* h);

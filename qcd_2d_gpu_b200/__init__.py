@@ -154,6 +154,8 @@ _SIGS = {
     "qcd_measure_aos_noalloc": (_I, [_P, _I, _I, _I, _I, _P, _P]),
     "qcd_set_schedule": (_I, [_P, _I]),
     "qcd_get_schedule": (_I, [_P]),
+    "qcd_set_pair_layout": (_I, [_P, _I]),
+    "qcd_get_pair_layout": (_I, [_P]),
     "qcd_wave_plan": (_I, [_P, _P, _I, _P, _P, _P]),
     "qcd_wave_selftest_timeout": (_I, [_P]),
     "qcd_set_wave_tuning": (_I, [_P, _I, _I, _I]),
@@ -291,6 +293,13 @@ class Lattice:
 
     def schedule(self) -> str:
         return _SCHED_NAME[self._lib.qcd_get_schedule(self._h)]
+
+    def set_pair_layout(self, on: bool) -> None:
+        """FP32, Lt % 4 == 0: allow (True, the default) or forbid the site-pair store."""
+        self._check(self._lib.qcd_set_pair_layout(self._h, int(bool(on))), "set_pair_layout")
+
+    def pair_layout(self) -> bool:
+        return self._lib.qcd_get_pair_layout(self._h) == 1
 
     def set_wave_tuning(self, chunk_sites: int = 0, passes_per_launch: int = 0, fronts: int = 0) -> None:
         self._check(self._lib.qcd_set_wave_tuning(self._h, chunk_sites, passes_per_launch, fronts),

@@ -13,6 +13,7 @@
 #include <new>
 #include <vector>
 #include "kernels.cuh"
+#include "paired.cuh"
 #include "pairs.h"
 #include "qcd2d.h"
 #include "wave.cuh"
@@ -31,6 +32,11 @@ struct qcd_lattice {
   float4* q32 = nullptr;     // FP32 store holding the current links
   float4* q32alt = nullptr;  // second FP32 store: the fused-pair schedule writes each pass's new links here
   size_t link_bytes = 0;
+  // FP32 store in site pairs (paired.cuh): FP32 lattices with Lt % 4 == 0 under
+  // the per-phase schedule; gh is the half geometry whose t-slices are its rows
+  bool paired = false;
+  bool pair_ok = true;  // qcd_set_pair_layout: pairs allowed
+  Geo gh;
   // MRG32k3a streams, 6 u32 planes, and the jump matrices that seed them
   uint32_t* rng = nullptr;
   uint32_t* mrg_jumps = nullptr;
@@ -106,6 +112,8 @@ inline unsigned int nblocks(long long n) { return (unsigned int)((n + kBlock - 1
 
 Links64 links64(const qcd_lattice* h) { return Links64{h->lo, h->hi, h->g.vh}; }
 Links32 links32(const qcd_lattice* h) { return Links32{h->q32, h->g.vh}; }
+Pair32 pair32(const qcd_lattice* h) { return Pair32{h->q32, h->g.vh / 2}; }
+bool pairable(const qcd_lattice* h) { return h->p.precision == QCD_PREC_FP32 && h->g.lt % 4 == 0; }
 RngStore rngs(const qcd_lattice* h) { return RngStore{h->rng, h->g.vh}; }
 
 // ------------------------------------------------------------ dispatch --
@@ -163,14 +171,43 @@ Phase32Fn phase_fn32(int k, int bc, int kind) {
   }
 }
 
+typedef void (*Phase32pFn)(Pair32, Geo, PhaseArgs);
+template <int MU, int PAR, int BC>
+Phase32pFn pick32p(int kind) {
+  switch (kind) {
+    case KIND_METRO: return phase32p<MU, PAR, BC, KIND_METRO>;
+    case KIND_HB: return phase32p<MU, PAR, BC, KIND_HB>;
+    default: return phase32p<MU, PAR, BC, KIND_OR>;
+  }
+}
+template <int MU, int PAR>
+Phase32pFn pick32p_bc(int bc, int kind) {
+  return bc == BC_PER ? pick32p<MU, PAR, BC_PER>(kind)
+         : bc == BC_PCC ? pick32p<MU, PAR, BC_PCC>(kind)
+                        : pick32p<MU, PAR, BC_PMC>(kind);
+}
+Phase32pFn phase_fn32p(int k, int bc, int kind) {
+  switch (k) {
+    case 0: return pick32p_bc<DIR_Y, 0>(bc, kind);
+    case 1: return pick32p_bc<DIR_Y, 1>(bc, kind);
+    case 2: return pick32p_bc<DIR_X, 0>(bc, kind);
+    case 3: return pick32p_bc<DIR_X, 1>(bc, kind);
+    case 4: return pick32p_bc<DIR_T, 0>(bc, kind);
+    default: return pick32p_bc<DIR_T, 1>(bc, kind);
+  }
+}
+
 // one pass over the six phases with one update kind; with `renorm` (FP32
 // only) every link is re-projected as it is stored
 int pass(qcd_lattice* h, int kind, int renorm = 0) {
   PhaseArgs a{h->p.beta, h->p.epsilon, h->p.upd, h->err, h->accept, renorm, h->draw_key, h->draw_dev, 0, 0, philox_keys(h->draw_key)};
   const dim3 grid(nblocks(h->g.slice), (unsigned int)h->g.lt);
+  const dim3 grid_p(nblocks(h->gh.slice), (unsigned int)h->gh.lt);
   for (int k = 0; k < 6; k++) {
     a.phase_off = (unsigned int)k;
-    if (h->p.precision == QCD_PREC_FP64)
+    if (h->paired)
+      phase_fn32p(k, h->p.boundary, kind)<<<grid_p, kBlock, 0, h->stream>>>(pair32(h), h->gh, a);
+    else if (h->p.precision == QCD_PREC_FP64)
       phase_fn64(k, h->p.boundary, kind)<<<grid, kBlock, 0, h->stream>>>(links64(h), rngs(h), h->g, a);
     else
       phase_fn32(k, h->p.boundary, kind)<<<grid, kBlock, 0, h->stream>>>(links32(h), rngs(h), h->g, a);
@@ -539,6 +576,11 @@ int launch_measure(qcd_lattice* h, double* out_dev) {
       measure<Links64, 1><<<nb, kBlock, 0, h->stream>>>(links64(h), h->g, h->partials, h->counter, out_dev);
     else
       measure<Links64, 0><<<nb, kBlock, 0, h->stream>>>(links64(h), h->g, h->partials, h->counter, out_dev);
+  } else if (h->paired) {
+    if (pmc)
+      measure_p<1><<<nb, kBlock, 0, h->stream>>>(pair32(h), h->gh, h->partials, h->counter, out_dev);
+    else
+      measure_p<0><<<nb, kBlock, 0, h->stream>>>(pair32(h), h->gh, h->partials, h->counter, out_dev);
   } else {
     if (pmc)
       measure<Links32, 1><<<nb, kBlock, 0, h->stream>>>(links32(h), h->g, h->partials, h->counter, out_dev);
@@ -672,6 +714,8 @@ int qcd_create(const qcd_params* p, qcd_lattice** out) {
   h->p = *p;
   h->V = V;
   h->g = make_geo(p->lt, p->lx, p->ly);
+  h->gh = make_geo(p->lt / 2, p->lx, p->ly);
+  h->paired = pairable(h);  // the store is written in pairs from the first start or load on
   h->draw_key = p->seed;
   const size_t vh = (size_t)h->g.vh;
   int rc = QCD_OK;
@@ -742,6 +786,8 @@ int qcd_init_cold(qcd_lattice* h) {
   if (!h) return QCD_ERR_INVALID;
   if (h->p.precision == QCD_PREC_FP64)
     init_cold<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(links64(h), h->g.vh);
+  else if (h->paired)
+    init_cold<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(pair32(h), h->g.vh);
   else
     init_cold<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(links32(h), h->g.vh);
   LAUNCH_CHECK(h);
@@ -755,6 +801,8 @@ int qcd_init_hot(qcd_lattice* h) {
   const int pcc = h->p.boundary == QCD_BC_PCC;
   if (h->p.precision == QCD_PREC_FP64)
     init_hot<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(links64(h), rngs(h), h->g, pcc);
+  else if (h->paired)
+    init_hot<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(pair32(h), rngs(h), h->g, pcc);
   else
     init_hot<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(links32(h), rngs(h), h->g, pcc);
   LAUNCH_CHECK(h);
@@ -770,6 +818,8 @@ int qcd_load_config_device(qcd_lattice* h, const double* aos_dev) {
   if (!h || !aos_dev) return QCD_ERR_INVALID;
   if (h->p.precision == QCD_PREC_FP64)
     aos_to_soa64<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(aos_dev, links64(h), h->g.vh);
+  else if (h->paired)
+    aos_to_pair32<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(aos_dev, pair32(h), h->g.vh);
   else
     aos_to_soa32<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(aos_dev, links32(h), h->g.vh);
   LAUNCH_CHECK(h);
@@ -780,6 +830,8 @@ int qcd_store_config_device(qcd_lattice* h, double* aos_dev) {
   if (!h || !aos_dev) return QCD_ERR_INVALID;
   if (h->p.precision == QCD_PREC_FP64)
     soa_to_aos64<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(links64(h), aos_dev, h->g.vh);
+  else if (h->paired)
+    pair32_to_aos<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(pair32(h), aos_dev, h->g.vh);
   else
     soa_to_aos32<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(links32(h), aos_dev, h->g.vh);
   LAUNCH_CHECK(h);
@@ -813,6 +865,8 @@ int qcd_normalize(qcd_lattice* h) {
   if (!h) return QCD_ERR_INVALID;
   if (h->p.precision == QCD_PREC_FP64)
     normalize64<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(links64(h), h->g.vh);
+  else if (h->paired)
+    normalize32p<<<nblocks(h->gh.vh), kBlock, 0, h->stream>>>(pair32(h));
   else
     normalize32<<<nblocks(h->g.vh), kBlock, 0, h->stream>>>(links32(h), h->g.vh);
   LAUNCH_CHECK(h);
@@ -861,6 +915,30 @@ int qcd_overrelax(qcd_lattice* h, int n) {
   return QCD_OK;
 }
 
+// The FP32 store rewritten in the other layout (site pairs <-> one float4
+// plane per class) through a scratch store; the links keep their values.
+int set_paired(qcd_lattice* h, bool paired) {
+  if (h->paired == paired) return QCD_OK;
+  if (paired && !pairable(h)) return fail(h, QCD_ERR_INVALID, "site pairs need an FP32 lattice with Lt %% 4 == 0");
+  float4* tmp = nullptr;
+  CUDA_OR_FAIL(h, cudaMalloc(&tmp, h->link_bytes));
+  cudaError_t e = cudaSuccess;
+  if (paired) {
+    e = cudaMemcpyAsync(tmp, h->q32, h->link_bytes, cudaMemcpyDeviceToDevice, h->stream);
+    if (e == cudaSuccess) plain_to_pair32<<<nblocks(h->gh.vh), kBlock, 0, h->stream>>>(tmp, pair32(h));
+  } else {
+    pair32_to_plain<<<nblocks(h->gh.vh), kBlock, 0, h->stream>>>(pair32(h), tmp);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->q32, tmp, h->link_bytes, cudaMemcpyDeviceToDevice, h->stream);
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(h, QCD_ERR_CUDA, "changing the FP32 store layout: %s", cudaGetErrorString(e));
+  h->paired = paired;
+  return QCD_OK;
+}
+
 int qcd_set_schedule(qcd_lattice* h, int mode) {
   if (!h || mode < QCD_SCHED_AUTO || mode > QCD_SCHED_PAIRS) return QCD_ERR_INVALID;
   if (mode == QCD_SCHED_PAIRS) {
@@ -869,8 +947,26 @@ int qcd_set_schedule(qcd_lattice* h, int mode) {
     int rc = pairs_setup(h);
     if (rc) return rc;
   }
+  // the per-phase schedule runs FP32 lattices with Lt % 4 == 0 on the paired
+  // store; the wavefront and the fused pairs read one float4 plane per class
+  if (h->p.precision == QCD_PREC_FP32) {
+    int rc = set_paired(h, pairable(h) && h->pair_ok && (mode == QCD_SCHED_AUTO || mode == QCD_SCHED_PHASES));
+    if (rc) return rc;
+  }
   h->sched = mode;
   return QCD_OK;
+}
+
+int qcd_set_pair_layout(qcd_lattice* h, int on) {
+  if (!h || on < 0 || on > 1) return QCD_ERR_INVALID;
+  h->pair_ok = on != 0;
+  if (h->p.precision != QCD_PREC_FP32) return QCD_OK;
+  return set_paired(h, pairable(h) && h->pair_ok && (h->sched == QCD_SCHED_AUTO || h->sched == QCD_SCHED_PHASES));
+}
+
+int qcd_get_pair_layout(const qcd_lattice* h) {
+  if (!h) return QCD_ERR_INVALID;
+  return h->paired ? 1 : 0;
 }
 
 int qcd_get_schedule(const qcd_lattice* h) {
@@ -989,6 +1085,7 @@ int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
   CUDA_OR_FAIL(h, cudaStreamSynchronize(h->stream));
   const int sched_save = h->sched, chunk_save = h->wave_chunk, chain_save = h->wave_chain, fronts_save = h->wave_fronts,
             pseg_save = h->pair_seg;
+  const bool paired_save = h->paired;  // the saved links are in this layout
   cudaEvent_t &e0 = bk.e0, &e1 = bk.e1;
   CUDA_OR_FAIL(h, cudaEventCreate(&e0));
   CUDA_OR_FAIL(h, cudaEventCreate(&e1));
@@ -1017,6 +1114,7 @@ int qcd_autotune(qcd_lattice* h, int sweeps_per_trial, qcd_tuning* chosen) {
   h->unit_passes = passes_save;
   h->sweeps_done = sweeps_save;
   h->sched = sched_save;
+  h->paired = paired_save;
   h->wave_chunk = chunk_save;
   h->wave_chain = chain_save;
   h->wave_fronts = fronts_save;
@@ -1136,6 +1234,8 @@ int qcd_check_unitarity(qcd_lattice* h, double tol, double* mean_det) {
   const unsigned int nb = nblocks(h->g.vh);
   if (h->p.precision == QCD_PREC_FP64)
     unitarity<<<nb, kBlock, 0, h->stream>>>(links64(h), h->g.vh, tol, h->partials, h->counter, h->result);
+  else if (h->paired)
+    unitarity_p<<<nblocks(h->gh.vh), kBlock, 0, h->stream>>>(pair32(h), tol, h->partials, h->counter, h->result);
   else
     unitarity<<<nb, kBlock, 0, h->stream>>>(links32(h), h->g.vh, tol, h->partials, h->counter, h->result);
   LAUNCH_CHECK(h);

@@ -1,4 +1,5 @@
-"""Batched replicas against single lattices (bit for bit) and the oracle."""
+"""Batched replicas against single lattices (bit for bit, on the store layout
+the replicas use: one float4 plane per link class) and the oracle."""
 import numpy as np
 import pytest
 
@@ -28,6 +29,7 @@ def test_batch_matches_single_lattices(precision, algo, n_or, graph):
     assert B.measured() == 6
     for i, r in enumerate(REPS):
         L = q.Lattice(r["lt"], r["lx"], r["ly"], r["beta"], boundary=r["boundary"], seed=r["seed"], **kw)
+        L.set_pair_layout(False)  # the replicas' store: one float4 plane per class
         L.init_hot() if r["hot"] else L.init_cold()
         ser = []
         for _ in range(6):
