@@ -493,6 +493,7 @@ def main():
     L.init_hot()
 
     L_schedule = L.schedule()
+    L_paired = L.pair_layout()  # FP32 with Lt % 4 == 0: the site-pair store and its kernels
 
     def step():
         L.sweep(N_COR)
@@ -568,6 +569,7 @@ def main():
     hbm, peak_kind = peaks()
     or_gbs = or_bytes / (or_launch_ms * 1e-3) / 1e9
     kname = ("pair32<mu, PMC, OR> (fused over-relaxation pair)" if L_schedule == "pairs"
+             else "phase32p<mu, par, PMC, OR> (over-relaxation phase, site-pair store)" if L_paired
              else f"phase{PREC[2:]}<mu, par, PMC, OR> (over-relaxation phase)")
     roofline = {"kernel": kname, "bound": "hbm", "achieved": or_gbs,
                 "peak": hbm, "unit": "GB/s", "frac": or_gbs / hbm, "peak_source": peak_kind,
@@ -577,7 +579,8 @@ def main():
     traffic_file = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(traffic_file) and PREC == "fp32" and L_schedule == "phases":
         try:
-            roofline["traffic"] = json.load(open(traffic_file)).get("phase32_or_bytes_per_launch")
+            key = "phase32p_or_bytes_per_launch" if L_paired else "phase32_or_bytes_per_launch"
+            roofline["traffic"] = json.load(open(traffic_file)).get(key)
         except Exception:
             pass
     if roofline["traffic"]:
