@@ -303,8 +303,10 @@ __global__ void __launch_bounds__(kBlock) measure_p(Pair32 P, Geo gh, double2* p
 }
 
 // ------------------------------------------------ whole-store kernels ----
+// (internal linkage: each translation unit that includes this header and
+// launches them has its own copy)
 // thread per pair: re-projection of both lanes of all six planes (normalize)
-__global__ void __launch_bounds__(kBlock) normalize32p(Pair32 P) {
+static __global__ void __launch_bounds__(kBlock) normalize32p(Pair32 P) {
   const int j = blockIdx.x * kBlock + threadIdx.x;
   if (j >= P.vhp) return;
   for (int p = 0; p < 2; p++)
@@ -315,7 +317,7 @@ __global__ void __launch_bounds__(kBlock) normalize32p(Pair32 P) {
 }
 
 // unitarity (kernels.cuh): thread per pair
-__global__ void __launch_bounds__(kBlock) unitarity_p(Pair32 P, double tol, double2* partials, unsigned int* counter,
+static __global__ void __launch_bounds__(kBlock) unitarity_p(Pair32 P, double tol, double2* partials, unsigned int* counter,
                                                       double* out) {
   const int j = blockIdx.x * kBlock + threadIdx.x;
   double s = 0, bad = 0;
@@ -338,7 +340,7 @@ __global__ void __launch_bounds__(kBlock) unitarity_p(Pair32 P, double tol, doub
 }
 
 // reference AoS (phi[(p*Vh + id)*12 + d*4 + c]) <-> paired store, thread per site
-__global__ void __launch_bounds__(kBlock) aos_to_pair32(const double* __restrict__ aos, Pair32 P, int vh) {
+static __global__ void __launch_bounds__(kBlock) aos_to_pair32(const double* __restrict__ aos, Pair32 P, int vh) {
   const int id = blockIdx.x * kBlock + threadIdx.x;
   if (id >= vh) return;
   for (int p = 0; p < 2; p++) {
@@ -348,7 +350,7 @@ __global__ void __launch_bounds__(kBlock) aos_to_pair32(const double* __restrict
                 Quat<float>{(float)s[d * 4 + 0], (float)s[d * 4 + 1], (float)s[d * 4 + 2], (float)s[d * 4 + 3]});
   }
 }
-__global__ void __launch_bounds__(kBlock) pair32_to_aos(Pair32 P, double* __restrict__ aos, int vh) {
+static __global__ void __launch_bounds__(kBlock) pair32_to_aos(Pair32 P, double* __restrict__ aos, int vh) {
   const int id = blockIdx.x * kBlock + threadIdx.x;
   if (id >= vh) return;
   for (int p = 0; p < 2; p++) {
@@ -364,7 +366,7 @@ __global__ void __launch_bounds__(kBlock) pair32_to_aos(Pair32 P, double* __rest
 }
 
 // one float4 plane store (Links32) <-> paired store, thread per pair
-__global__ void __launch_bounds__(kBlock) plain_to_pair32(const float4* __restrict__ src, Pair32 P) {
+static __global__ void __launch_bounds__(kBlock) plain_to_pair32(const float4* __restrict__ src, Pair32 P) {
   const int j = blockIdx.x * kBlock + threadIdx.x;
   if (j >= P.vhp) return;
   for (int k = 0; k < 6; k++) {
@@ -374,7 +376,7 @@ __global__ void __launch_bounds__(kBlock) plain_to_pair32(const float4* __restri
     d[1] = make_float4(a.z, b.z, a.w, b.w);
   }
 }
-__global__ void __launch_bounds__(kBlock) pair32_to_plain(Pair32 P, float4* __restrict__ dst) {
+static __global__ void __launch_bounds__(kBlock) pair32_to_plain(Pair32 P, float4* __restrict__ dst) {
   const int j = blockIdx.x * kBlock + threadIdx.x;
   if (j >= P.vhp) return;
   for (int k = 0; k < 6; k++) {
