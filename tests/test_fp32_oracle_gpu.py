@@ -48,13 +48,18 @@ def counter_and_key(L):
     return int(w[-4]) | (int(w[-3]) << 32), int(w[-2]) | (int(w[-1]) << 32)
 
 
-SCHEDULES = ["phases", "pairs"]
+# "phases" runs lattices with Lt % 4 == 0 on the site-pair store (the default),
+# "phases-planes" the same per-phase launches on one float4 plane per class
+SCHEDULES = ["phases", "phases-planes", "pairs"]
 
 
 def thermalised(dims, bc, beta, algo="hb", seed=7, schedule="phases", **kw):
     L = q.Lattice(*dims, beta, algo=algo, boundary=bc, precision="fp32", seed=seed, **kw)
     L.init_hot()
     L.sweep(4)
+    if schedule == "phases-planes":
+        L.set_pair_layout(False)
+        schedule = "phases"
     L.set_schedule(schedule)  # the pass under test runs with this schedule
     return L
 

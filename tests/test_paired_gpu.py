@@ -133,3 +133,23 @@ def test_paired_sweeps_track_unpaired_statistically():
     m = [x.mean() for x in res]
     err = [x.std(ddof=1) / np.sqrt(len(x) / 10.0) for x in res]  # generous: tau_int <= 5
     assert abs(m[0] - m[1]) <= 4 * np.hypot(*err), (m, err)
+
+
+def test_autotune_on_the_pair_store_restores_links_layout_and_counters():
+    # the candidates include schedules that rewrite the store into float4
+    # planes; the tuner puts back the links, their layout and the draw counter
+    kw = dict(boundary=2, precision="fp32", n_or=1, renorm_every=1, seed=21)
+    a = q.Lattice(12, 10, 14, 7.0, **kw)
+    b = q.Lattice(12, 10, 14, 7.0, **kw)
+    for L in (a, b):
+        L.init_hot()
+        L.sweep(2)
+    t = a.autotune(1)
+    assert np.array_equal(a.store_config(), b.store_config())
+    assert a.pair_layout() == (t["schedule"] == "phases")
+    a.set_schedule("phases")
+    b.set_schedule("phases")
+    assert a.pair_layout() and b.pair_layout()
+    a.sweep(2)
+    b.sweep(2)
+    assert np.array_equal(a.store_config(), b.store_config())
