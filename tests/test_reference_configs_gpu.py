@@ -5,8 +5,8 @@ kernels (oracle/_ref/ref_harness, built from its sources for sm_100a) run at
 the full sizes of the benchmark configurations, and the FP64 path is
 compared with them field for field:
   C2  32x32x64, PCC, beta 8, hot, Metropolis eps 0.2 upd 4 (the full config);
-  C3  the PMC heat-bath sweep at 96^3 (the 384^3 lattice's link dumps would
-      be 5.4 GB each; the sweep, its boundary and its streams are the same);
+  C3  the PMC heat-bath sweep at 96^3 over ten sweeps, and on the 384^3
+      lattice itself over two (its field dump is 5.4 GB);
   C5  128^3 periodic heat-bath from a cold start at beta 4.
 Heat-bath fields must agree bit for bit, Metropolis to the few ulp its
 proposal arithmetic contracts differently (with identical accept arrays);
@@ -65,3 +65,54 @@ def test_fp64_path_matches_the_reference_kernels_at_benchmark_sizes(cfg, tmp_pat
     assert np.abs(np.array(mine) - obs).max() <= 1e-13
     assert np.array_equal(L.accept_counts(), acc)
     L.close()
+
+
+def _dump_dir(tmp_path, need):
+    import shutil
+
+    for d in ("/dev/shm", str(tmp_path)):
+        try:
+            if os.path.isdir(d) and os.access(d, os.W_OK) and shutil.disk_usage(d).free >= need:
+                return d
+        except OSError:
+            pass
+    return None
+
+
+def test_fp64_path_matches_the_reference_kernels_at_the_headline_size(tmp_path):
+    """C3's lattice itself (384^3, PMC, beta 10, hot start): two heat-bath
+    sweeps of the reference's kernels and of the FP64 path, bit for bit (the
+    reference's field dump is 5.4 GB, written where there is room for it)."""
+    if not os.path.exists(REF_HARNESS):
+        pytest.skip("reference harness not built (needs the reference checkout at build time)")
+    lt = lx = ly = 384
+    sweeps = 2
+    V = lt * lx * ly
+    d = _dump_dir(tmp_path, 12 * 2**30)
+    if d is None:
+        pytest.skip("no directory with 12 GB free for the 5.4 GB reference field dump")
+    pre = os.path.join(d, f"qcd2d_c3_384_{os.getpid()}")
+    try:
+        out = subprocess.run(
+            [REF_HARNESS, "run", "--lt", str(lt), "--lx", str(lx), "--ly", str(ly), "--algo", "hb", "--bc", "2",
+             "--hot", "1", "--beta", "10.0", "--seed", "1234", "--sweeps", str(sweeps), "--dumps", str(sweeps),
+             "--out", pre],
+            capture_output=True, text=True, timeout=900)
+        assert out.returncode == 0, out.stderr
+        ref = np.fromfile(f"{pre}_field_{sweeps}.bin", dtype=np.float64)
+        obs = np.fromfile(f"{pre}_obs.bin", dtype=np.float64).reshape(sweeps, 2)
+    finally:
+        for suffix in (f"_field_{sweeps}.bin", "_obs.bin", "_accept.bin"):
+            if os.path.exists(pre + suffix):
+                os.remove(pre + suffix)
+    assert ref.size == V * 12
+    L = q.Lattice(lt, lx, ly, 10.0, algo="hb", boundary=2, seed=1234)
+    L.init_hot()
+    mine = []
+    for _ in range(sweeps):
+        L.sweep(1)
+        mine.append(L.measure())
+    field = L.store_config()
+    L.close()
+    assert np.array_equal(field, ref), "heat-bath must be bit-identical"
+    assert np.abs(np.array(mine) - obs).max() <= 1e-13
