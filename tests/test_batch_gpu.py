@@ -129,3 +129,36 @@ def test_batch_autotune_restores_the_batch():
         assert np.array_equal(A.store_config(i), T.store_config(i))
     A.close()
     T.close()
+
+
+def test_c4_batch_matches_lone_lattices():
+    # the benchmark's 96 replicas (shapes 8^3 to 64x64x128, beta in [3, 12],
+    # boundary r mod 3, hot for even r), each with a seed of its own so that a
+    # lone lattice (whose streams start at 0) can reproduce it; FP32 heat-bath
+    # re-projected every sweep, grouped on lanes as the benchmark runs them:
+    # every replica's links and series are those of the same lattice run alone
+    import bench
+
+    reps = [dict(r, seed=1234 + i, stream_offset=0) for i, r in enumerate(bench.c4_replicas())]
+    sweeps = 4
+    kw = dict(algo="hb", precision="fp32", renorm_every=1)
+    B = q.Batch(reps, **kw)
+    B.set_groups(16 << 20)
+    B.set_lanes(4)
+    B.init()
+    B.reserve(sweeps)
+    B.run(sweeps, measure_every=1, graph=True)
+    assert B.measured() == sweeps
+    for i, r in enumerate(reps):
+        L = q.Lattice(r["lt"], r["lx"], r["ly"], r["beta"], boundary=r["boundary"], seed=r["seed"], **kw)
+        L.set_pair_layout(False)  # the replicas' store: one float4 plane per class
+        L.init_hot() if r["hot"] else L.init_cold()
+        ser = []
+        for _ in range(sweeps):
+            L.sweep(1)
+            ser.append(L.measure())
+        e, p = B.series(i, sweeps)
+        assert np.array_equal(e, [s[0] for s in ser]) and np.array_equal(p, [s[1] for s in ser]), i
+        assert np.array_equal(B.store_config(i), L.store_config()), i
+        L.close()
+    B.close()
