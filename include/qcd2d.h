@@ -177,7 +177,8 @@ int qcd_get_schedule(const qcd_lattice* h);
    site pairs under the per-phase schedule: site id (t < Lt/2) and site
    id + V/4 (t + Lt/2) of a link class share one 32-B record (w0 w1 x0 x1)
    (y0 y1 z0 z1), and one thread updates both with packed two-lane FP32
-   arithmetic (about half the instructions per link update).  Same updates
+   arithmetic (20-30% fewer instructions per link update; each quaternion
+   product takes half).  Same updates
    and draws as one float4 plane per class; results agree with it to float
    rounding.  on = 0 keeps such a lattice on one float4 plane per class (the
    layout of the wavefront and fused-pair schedules and of the batched
@@ -198,11 +199,13 @@ int qcd_set_pair_tuning(qcd_lattice* h, int slices_per_cta);
    ready tasks and the live slices).  Defaults: 256 sites, as many passes as
    keep the live slices within ~64 MB, 1 front. */
 int qcd_set_wave_tuning(qcd_lattice* h, int chunk_sites, int passes_per_launch, int fronts);
-/* Autotuner.  Times per-phase launches and the wavefront (task sizes 256 /
-   512 / 1024 sites, 1..32 fronts whose live slices fit in L2, 1 or the
-   largest chain of passes) for sweeps_per_trial sweeps each (0: 2) on this
-   lattice, then restores the lattice's links, streams and counters exactly
-   and keeps the fastest schedule.  The choice is cached per (extents,
+/* Autotuner.  Times per-phase launches, the fused pairs (FP32) and the
+   wavefront (task sizes 256 / 512 / 1024 sites, 1..32 fronts whose live
+   slices fit in L2, 1 or the largest chain of passes) for sweeps_per_trial
+   sweeps each (0: 2) on this lattice (per-phase on the site-pair store where
+   it applies, the others on float4 planes), then restores the lattice's
+   links, their layout, streams and counters exactly and keeps the fastest
+   schedule.  The choice is cached per (extents,
    precision, algorithm, boundary, n_or) for the life of the process, so later
    handles of the same shape reuse it without timing. */
 typedef struct qcd_tuning {
