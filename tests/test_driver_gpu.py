@@ -25,6 +25,8 @@ RUNS = [
     ("hb", 8, 8, 8, 6.0, 0, 1, 20, 30, 2, 3, 5, 0.1, 1),
     ("hb", 6, 4, 8, 9.0, 2, 0, 12, 20, 1, 2, 4, 0.1, 1),
     ("metro", 8, 8, 16, 8.0, 1, 0, 15, 24, 3, 4, 6, 0.2, 4),
+    # C1 of the benchmark configurations: 16^3 periodic, beta 6, cold start, N_term 200, N 100, N_cor 5
+    ("hb", 16, 16, 16, 6.0, 0, 1, 200, 100, 5, 4, 10, 0.1, 1),
 ]
 
 
@@ -82,7 +84,7 @@ def compare_dirs(a, b, algo):
             assert same_text(open(pa).read(), open(pb).read()), name
 
 
-@pytest.mark.parametrize("r", RUNS, ids=lambda r: f"{r[0]}_bc{r[5]}")
+@pytest.mark.parametrize("r", RUNS, ids=lambda r: f"{r[0]}_bc{r[5]}_{r[1]}x{r[2]}x{r[3]}")
 def test_driver_leaves_the_reference_files(r, tmp_path):
     if not os.path.exists(HARNESS):
         pytest.skip("reference harness not built (needs the reference checkout at build time)")
