@@ -238,11 +238,12 @@ __device__ __forceinline__ Q2 pair_update(const PS& P, const Geo& gh, const Phas
   return U;
 }
 
-// Launch grid (ceil(slice / kBlock), Lt/2): blockIdx.y is the row.  Five
-// CTAs per SM (48 registers) for over-relaxation and Metropolis; the
-// heat-bath runs spill-free at four (64 registers), measured faster.
+// Launch grid (ceil(slice / kBlock), Lt/2): blockIdx.y is the row.  The
+// heat-bath and over-relaxation phases run spill-free at four CTAs per SM (64
+// registers), measured 3-5% faster than five with small spills; Metropolis
+// keeps five.
 template <int MU, int PAR, int BC, int KIND>
-__global__ void __launch_bounds__(kBlock, KIND == KIND_HB ? 4 : 5) phase32p(Pair32 P, Geo gh, PhaseArgs a) {
+__global__ void __launch_bounds__(kBlock, KIND == KIND_METRO ? 5 : 4) phase32p(Pair32 P, Geo gh, PhaseArgs a) {
   const int s = blockIdx.x * kBlock + threadIdx.x;
   if (s >= gh.slice) return;
   const int r = blockIdx.y;
